@@ -1,0 +1,129 @@
+/* remora_cuda.h -- the C-ABI of libremora_cuda.so, the sm_100a (B200) kernels behind
+ * Remora's `cuda_tag` device.
+ *
+ * Conventions (the cuBLAS-style column-major convention that the reference's HIP
+ * backend maps every orientation onto, include/remora/kernels/hip/gemm.hpp:46-88):
+ *  - matrices are column-major with a leading dimension; `trans*` flags select op(X) = X
+ *    or X^T. A row-major matrix is passed as its transpose (swap the dimensions, flip
+ *    the flag), exactly as the reference's row-major overloads do;
+ *  - all pointers are device pointers unless stated; every call is asynchronous on the
+ *    caller's `stream` (a cudaStream_t; NULL = the legacy default stream);
+ *  - the return value is a status (RC_SUCCESS = 0); numerical outcomes that are only
+ *    known on the device (a failing pivot, a zero diagonal) are written to a
+ *    caller-provided device int `d_info` (may be NULL where stated);
+ *  - the library allocates only internal workspaces, cached per device and stream
+ *    (released by rc_release_workspaces).
+ */
+#ifndef REMORA_CUDA_H
+#define REMORA_CUDA_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    RC_SUCCESS = 0,
+    RC_ERR_INVALID_ARGUMENT = 1, /* a size, leading dimension or flag is out of range */
+    RC_ERR_CUDA = 2,             /* a CUDA runtime call or kernel launch failed */
+    RC_ERR_ALLOC = 3,            /* a workspace allocation failed */
+    RC_ERR_NOT_SUPPORTED = 4,    /* a combination the library does not implement */
+    RC_ERR_TIMEOUT = 5,          /* a bounded device-side wait gave up */
+    RC_ERR_NOT_CONVERGED = 6     /* iterative refinement did not reach its tolerance */
+};
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int rc_version(void);
+/* Static description of a status code. */
+const char* rc_error_string(int status);
+/* Free every cached workspace of the current device (synchronises the device). */
+int rc_release_workspaces(void);
+
+/* ---------------------------------------------------------------------------------
+ * Counter-based RNG fills of a rows x cols float/int matrix (Threefry-4x32, 12 rounds).
+ * Replaces bindings::generate_normal/uniform/discrete for hip_tag,
+ * include/remora/kernels/hip/random.hpp:218-323 (kernels :163-210, generator :40-161).
+ * key: the 4 words the reference draws from the host generator (:225-227).
+ * Element (i, j) is component j % 4 of Threefry(ctr(i, 4*floor(j/4)), key) with
+ * ctr(i, j) = (i & 0xffff, i >> 32, j & 0xffff, j >> 32) (:167), independent of storage
+ * order; row_major selects the layout of A (leading dimension ld). Elements outside
+ * rows x cols are never written (the reference writes past the end, :172, :186). */
+int rc_rng_bits_u32(const uint32_t key[4], size_t rows, size_t cols, uint32_t* A, size_t ld,
+                    int row_major, void* stream);
+int rc_rng_uniform_f32(const uint32_t key[4], size_t rows, size_t cols, float* A, size_t ld,
+                       int row_major, float low, float high, void* stream);
+int rc_rng_normal_f32(const uint32_t key[4], size_t rows, size_t cols, float* A, size_t ld,
+                      int row_major, float mean, float stddev, void* stream);
+/* Discrete values low + (x % (high - low + 1)); requires low <= high and a range below 2^32. */
+int rc_rng_discrete_f32(const uint32_t key[4], size_t rows, size_t cols, float* A, size_t ld,
+                        int row_major, int low, int high, void* stream);
+int rc_rng_discrete_i32(const uint32_t key[4], size_t rows, size_t cols, int32_t* A, size_t ld,
+                        int row_major, int low, int high, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * C <- alpha * op(A) * op(B) + beta * C, C m x n, op(A) m x k, op(B) k x n.
+ * Replaces kernels::gemm for hip_tag (include/remora/kernels/hip/gemm.hpp:46-112 ->
+ * include/remora/hip/cublas_backend.hpp:121-166). beta == 0 does not read C.
+ * rc_gemm_f64: FP64 on the DMMA tensor path; rc_gemm_f32: FP32-accurate. */
+int rc_gemm_f64(int transA, int transB, size_t m, size_t n, size_t k, double alpha,
+                const double* A, size_t lda, const double* B, size_t ldb, double beta,
+                double* C, size_t ldc, void* stream);
+int rc_gemm_f32(int transA, int transB, size_t m, size_t n, size_t k, float alpha,
+                const float* A, size_t lda, const float* B, size_t ldb, float beta,
+                float* C, size_t ldc, void* stream);
+
+/* C_tri <- alpha * op(A) * op(A)^T + beta * C_tri on the upper or lower triangle of the
+ * n x n matrix C; op(A) is n x k (trans = 0: A is n x k; trans = 1: A is k x n). The
+ * other triangle is not touched. Replaces kernels::syrk for hip_tag
+ * (include/remora/kernels/hip/syrk.hpp:44-85 -> hip/cublas_backend.hpp:389-431). */
+int rc_syrk_f64(int upper, int trans, size_t n, size_t k, double alpha, const double* A,
+                size_t lda, double beta, double* C, size_t ldc, void* stream);
+int rc_syrk_f32(int upper, int trans, size_t n, size_t k, float alpha, const float* A,
+                size_t lda, float beta, float* C, size_t ldc, void* stream);
+
+/* Triangular solve with m x n B: left: B <- alpha * op(A)^-1 B (A m x m);
+ * right: B <- alpha * B op(A)^-1 (A n x n). upper names the stored triangle of A,
+ * unit assumes a unit diagonal. d_info (may be NULL): set to 0, or to the 1-based index
+ * of the first exactly-zero diagonal element of A when !unit (the reference CPU kernel
+ * throws there, include/remora/kernels/default/trsm.hpp:86-87).
+ * Replaces kernels::trsm for hip_tag (include/remora/kernels/hip/trsm.hpp:45-107 ->
+ * hip/cublas_backend.hpp:303-344). */
+int rc_trsm_f64(int left, int upper, int trans, int unit, size_t m, size_t n, double alpha,
+                const double* A, size_t lda, double* B, size_t ldb, int* d_info, void* stream);
+int rc_trsm_f32(int left, int upper, int trans, int unit, size_t m, size_t n, float alpha,
+                const float* A, size_t lda, float* B, size_t ldb, int* d_info, void* stream);
+
+/* In-place Cholesky of the lower (A = L L^T) or upper (A = U^T U) triangle of the n x n
+ * column-major A; the opposite triangle is never written. d_info (required): set to 0 on
+ * success, else to the GLOBAL 1-based index of the first pivot that is not positive
+ * (the reference CPU kernel returns an index relative to its recursive sub-block,
+ * include/remora/kernels/default/potrf.hpp:125-133; the HIP kernel always returns 0,
+ * kernels/hip/potrf.hpp:139). Replaces kernels::potrf for hip_tag
+ * (include/remora/kernels/hip/potrf.hpp:41-141). */
+int rc_potrf_f64(int upper, size_t n, double* A, size_t lda, int* d_info, void* stream);
+int rc_potrf_f32(int upper, size_t n, float* A, size_t lda, int* d_info, void* stream);
+
+/* X = A^-1 B for SPD A via Cholesky: cholesky_decomposition(A).solve(B, left())
+ * (include/remora/decompositions.hpp:81-84, :101-105; solve.hpp:165-170). A (n x n,
+ * lower triangle read) is not modified; B (n x nrhs) is overwritten with X. d_info as
+ * in rc_potrf_*; on failure B is left unchanged. */
+int rc_spd_solve_f64(size_t n, size_t nrhs, const double* A, size_t lda, double* B, size_t ldb,
+                     int* d_info, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * Assignment support for the containers (include/remora/kernels/hip/matrix_assign.hpp:
+ * 38-200, include/remora/hip/dense.hpp:39-51, hip/buffer.hpp:105-125).
+ * rc_copy2d_*: B <- alpha * op(A) (A m x n if !trans, n x m if trans; B m x n).
+ * rc_fill_*: every element of the m x n matrix set to value. */
+int rc_copy2d_f64(int trans, size_t m, size_t n, double alpha, const double* A, size_t lda,
+                  double* B, size_t ldb, void* stream);
+int rc_copy2d_f32(int trans, size_t m, size_t n, float alpha, const float* A, size_t lda,
+                  float* B, size_t ldb, void* stream);
+int rc_fill_f64(size_t m, size_t n, double value, double* A, size_t lda, void* stream);
+int rc_fill_f32(size_t m, size_t n, float value, float* A, size_t lda, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* REMORA_CUDA_H */

@@ -1,0 +1,86 @@
+"""ctypes binding of libremora_cuda.so, the C-ABI declared in include/remora_cuda.h.
+
+This is the Python view of the same entry points a C++ host (the ``remora/cuda.hpp``
+headers) binds. Loading fails loudly when the library has not been built: there is no
+fallback path.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_double, c_float, c_int, c_size_t, c_uint32, c_void_p
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libremora_cuda.so"
+
+RC_SUCCESS = 0
+STATUS_NAMES = {0: "RC_SUCCESS", 1: "RC_ERR_INVALID_ARGUMENT", 2: "RC_ERR_CUDA", 3: "RC_ERR_ALLOC",
+                4: "RC_ERR_NOT_SUPPORTED", 5: "RC_ERR_TIMEOUT", 6: "RC_ERR_NOT_CONVERGED"}
+
+_U4 = POINTER(c_uint32)
+_I = c_int
+_Z = c_size_t
+_P = c_void_p
+
+# name -> argument types (restype is int for every entry point unless listed in _RESTYPES)
+SIGNATURES: dict[str, list] = {
+    "rc_version": [],
+    "rc_error_string": [_I],
+    "rc_release_workspaces": [],
+    "rc_rng_bits_u32": [_U4, _Z, _Z, _P, _Z, _I, _P],
+    "rc_rng_uniform_f32": [_U4, _Z, _Z, _P, _Z, _I, c_float, c_float, _P],
+    "rc_rng_normal_f32": [_U4, _Z, _Z, _P, _Z, _I, c_float, c_float, _P],
+    "rc_rng_discrete_f32": [_U4, _Z, _Z, _P, _Z, _I, _I, _I, _P],
+    "rc_rng_discrete_i32": [_U4, _Z, _Z, _P, _Z, _I, _I, _I, _P],
+    "rc_gemm_f64": [_I, _I, _Z, _Z, _Z, c_double, _P, _Z, _P, _Z, c_double, _P, _Z, _P],
+    "rc_gemm_f32": [_I, _I, _Z, _Z, _Z, c_float, _P, _Z, _P, _Z, c_float, _P, _Z, _P],
+    "rc_syrk_f64": [_I, _I, _Z, _Z, c_double, _P, _Z, c_double, _P, _Z, _P],
+    "rc_syrk_f32": [_I, _I, _Z, _Z, c_float, _P, _Z, c_float, _P, _Z, _P],
+    "rc_trsm_f64": [_I, _I, _I, _I, _Z, _Z, c_double, _P, _Z, _P, _Z, _P, _P],
+    "rc_trsm_f32": [_I, _I, _I, _I, _Z, _Z, c_float, _P, _Z, _P, _Z, _P, _P],
+    "rc_potrf_f64": [_I, _Z, _P, _Z, _P, _P],
+    "rc_potrf_f32": [_I, _Z, _P, _Z, _P, _P],
+    "rc_spd_solve_f64": [_Z, _Z, _P, _Z, _P, _Z, _P, _P],
+    "rc_copy2d_f64": [_I, _Z, _Z, c_double, _P, _Z, _P, _Z, _P],
+    "rc_copy2d_f32": [_I, _Z, _Z, c_float, _P, _Z, _P, _Z, _P],
+    "rc_fill_f64": [_Z, _Z, c_double, _P, _Z, _P],
+    "rc_fill_f32": [_Z, _Z, c_float, _P, _Z, _P],
+}
+_RESTYPES = {"rc_error_string": ctypes.c_char_p}
+
+_lib = None
+
+
+class RemoraCudaError(RuntimeError):
+    def __init__(self, name: str, status: int):
+        self.status = status
+        super().__init__(f"{name} returned {STATUS_NAMES.get(status, status)}: {error_string(status)}")
+
+
+def lib() -> ctypes.CDLL:
+    """Load libremora_cuda.so once (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m remora_b200.build`")
+        handle = ctypes.CDLL(str(LIB_PATH))
+        for name, argtypes in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.argtypes = argtypes
+            fn.restype = _RESTYPES.get(name, c_int)
+        _lib = handle
+    return _lib
+
+
+def error_string(status: int) -> str:
+    return lib().rc_error_string(status).decode()
+
+
+def call(name: str, *args) -> None:
+    """Call an entry point and raise RemoraCudaError on a non-zero status."""
+    status = getattr(lib(), name)(*args)
+    if status != RC_SUCCESS:
+        raise RemoraCudaError(name, status)
+
+
+def key_array(key) -> ctypes.Array:
+    return (c_uint32 * 4)(*[int(k) & 0xFFFFFFFF for k in key])

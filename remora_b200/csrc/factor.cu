@@ -1,0 +1,278 @@
+// Blocked triangular solve (TRSM) and blocked right-looking Cholesky (POTRF).
+//
+// Replaces kernels::trsm / kernels::potrf for hip_tag (include/remora/kernels/hip/
+// trsm.hpp:45-107 -> cublas trsm; include/remora/kernels/hip/potrf.hpp:41-141, a
+// recursive split whose 16x16 leaves are factored by a single thread). Here:
+//  * TRSM: every 128x128 diagonal block of the triangle is inverted at once (one CTA
+//    per block, FP64 in shared memory); the solve then walks the block rows, each step
+//    one GEMM with the inverted block and one GEMM update of the remaining rows, so
+//    nearly all flops run in the tensor-core GEMM.
+//  * POTRF: per 128-wide panel, one CTA factors the diagonal block in FP64 shared
+//    memory (and inverts it), the panel below is solved by a GEMM with that inverse,
+//    and the trailing matrix is updated by a lower-masked GEMM (the SYRK schedule).
+//    A non-positive pivot writes its global index to the status word and every later
+//    kernel of the factorization returns at once.
+#include "factor.cuh"
+#include "assign.cuh"
+#include "gemm.cuh"
+#include <type_traits>
+
+namespace rc {
+namespace {
+
+constexpr int NB = kNB;
+constexpr int SLD = NB + 1;  // shared-memory row stride (doubles)
+constexpr size_t kBlockSmem = (size_t)NB * SLD * sizeof(double);
+
+__device__ __forceinline__ bool aborted(const int* abort) { return abort != nullptr && *(volatile const int*)abort != 0; }
+
+// In-place inversion of the unit/non-unit lower-triangular NB x NB matrix in S
+// (row-major, stride SLD), one thread per column: row i of the inverse only needs row i
+// of L and the rows < i of the inverse in the thread's own column.
+__device__ void invert_lower_inplace(double* S, bool unit) {
+    const int j = threadIdx.x;
+    for (int i = 0; i < NB; ++i) {
+        double x = 0.0;
+        if (j <= i && j < NB) {
+            const double dinv = unit ? 1.0 : 1.0 / S[i * SLD + i];
+            if (j == i) {
+                x = dinv;
+            } else {
+                double a0 = 0.0, a1 = 0.0;
+                int k = j;
+                for (; k + 1 < i; k += 2) {
+                    a0 = fma(S[i * SLD + k], S[k * SLD + j], a0);
+                    a1 = fma(S[i * SLD + k + 1], S[(k + 1) * SLD + j], a1);
+                }
+                if (k < i) a0 = fma(S[i * SLD + k], S[k * SLD + j], a0);
+                x = -(a0 + a1) * dinv;
+            }
+        }
+        __syncthreads();
+        if (j <= i && j < NB) S[i * SLD + j] = x;
+    }
+    __syncthreads();
+}
+
+// Store the inverse (lower, zero above the diagonal) as a column-major NB x NB block.
+template <class T>
+__device__ void store_block(const double* S, T* W) {
+    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+        const int i = e % NB, j = e / NB;
+        W[e] = j <= i ? (T)S[i * SLD + j] : T(0);
+    }
+}
+
+// One CTA per diagonal block: W_b = inverse of the lower-triangular block b of L.
+template <class T>
+__global__ void __launch_bounds__(NB) trtri_blocks(int64_t m, View<const T> L, bool unit, T* W, int* info,
+                                                   const int* abort) {
+    extern __shared__ double S[];
+    if (aborted(abort)) return;
+    const int64_t r0 = (int64_t)blockIdx.x * NB;
+    const int sz = (int)(m - r0 < NB ? m - r0 : NB);
+    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+        const int i = e % NB, j = e / NB;
+        double v;
+        if (i < sz && j < sz && j <= i) v = (i == j && unit) ? 1.0 : (double)L(r0 + i, r0 + j);
+        else v = (i == j) ? 1.0 : 0.0;
+        S[i * SLD + j] = v;
+    }
+    __syncthreads();
+    if (!unit && info != nullptr && threadIdx.x < sz && S[threadIdx.x * SLD + threadIdx.x] == 0.0)
+        record_first(info, (int)(r0 + threadIdx.x + 1));
+    invert_lower_inplace(S, unit);
+    store_block<T>(S, W + (size_t)blockIdx.x * NB * NB);
+}
+
+// Factor the sz x sz lower diagonal block (A already offset to it) in FP64 shared
+// memory, write L back, and store inv(L) into W. g0 = global index of the block.
+template <class T>
+__global__ void __launch_bounds__(256) potrf_diag(View<T> A, int sz, int64_t g0, T* W, int* info) {
+    extern __shared__ double S[];
+    if (aborted(info)) return;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < NB * NB; e += blockDim.x) {
+        const int i = e % NB, j = e / NB;
+        S[i * SLD + j] = (i < sz && j < sz && j <= i) ? (double)A(i, j) : (i == j ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    for (int j = 0; j < sz; ++j) {
+        const double d = S[j * SLD + j];
+        if (!(d > 0.0)) {  // also catches NaN
+            if (tid == 0) record_first(info, (int)(g0 + j + 1));
+            return;
+        }
+        const double sq = sqrt(d);
+        __syncthreads();
+        for (int i = j + tid; i < sz; i += blockDim.x) S[i * SLD + j] = (i == j) ? sq : S[i * SLD + j] / sq;
+        __syncthreads();
+        const int t = sz - j - 1;
+        for (int e = tid; e < t * t; e += blockDim.x) {
+            const int i = j + 1 + e / t, c = j + 1 + e % t;
+            if (c <= i) S[i * SLD + c] = fma(-S[i * SLD + j], S[c * SLD + j], S[i * SLD + c]);
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < NB * NB; e += blockDim.x) {
+        const int i = e % NB, j = e / NB;
+        if (i < sz && j <= i) A(i, j) = (T)S[i * SLD + j];
+    }
+    __syncthreads();
+    invert_lower_inplace(S, false);
+    store_block<T>(S, W);
+}
+
+template <class K>
+int set_smem(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess
+               ? RC_SUCCESS
+               : RC_ERR_CUDA;
+}
+
+}  // namespace
+
+template <class T>
+int trsm_left(bool upper, bool unit, int64_t m, int64_t n, T alpha, View<const T> A, View<T> B, int* info,
+              cudaStream_t s, const int* abort) {
+    if (m <= 0 || n <= 0) return RC_SUCCESS;
+    const int64_t nblk = (m + NB - 1) / NB;
+    T* W = static_cast<T*>(workspace(s, (size_t)nblk * NB * NB * sizeof(T), 1));
+    T* tmp = static_cast<T*>(workspace(s, (size_t)NB * n * sizeof(T), 2));
+    if (!W || !tmp) return RC_ERR_ALLOC;
+    const View<const T> L = upper ? A.t() : A;
+    RC_TRY(set_smem(trtri_blocks<T>, kBlockSmem));
+    trtri_blocks<T><<<(unsigned)nblk, NB, kBlockSmem, s>>>(m, L, unit, W, info, abort);
+    RC_TRY(check_launch());
+    if (alpha != T(1)) RC_TRY(copy2d<T, T>(m, n, alpha, View<const T>{B.p, B.rs, B.cs}, B, s, abort));
+    const View<T> Tv = colmajor(tmp, (int64_t)NB);
+    for (int64_t step = 0; step < nblk; ++step) {
+        const int64_t b = upper ? nblk - 1 - step : step;
+        const int64_t r0 = b * NB, sz = (m - r0 < NB) ? m - r0 : NB;
+        const View<const T> X = {W + (size_t)b * NB * NB, 1, NB};
+        View<T> Bb = B.sub(r0, 0);
+        RC_TRY(gemm<T>(sz, n, sz, T(1), upper ? X.t() : X, View<const T>{Bb.p, Bb.rs, Bb.cs}, T(0), Tv, kFull, 0, s,
+                       abort));
+        RC_TRY(copy2d<T, T>(sz, n, T(1), View<const T>{Tv.p, Tv.rs, Tv.cs}, Bb, s, abort));
+        const View<const T> Bc = {Bb.p, Bb.rs, Bb.cs};
+        if (!upper && r0 + sz < m)
+            RC_TRY(gemm<T>(m - r0 - sz, n, sz, T(-1), A.sub(r0 + sz, r0), Bc, T(1), B.sub(r0 + sz, 0), kFull, 0, s,
+                           abort));
+        if (upper && r0 > 0) RC_TRY(gemm<T>(r0, n, sz, T(-1), A.sub(0, r0), Bc, T(1), B, kFull, 0, s, abort));
+    }
+    return RC_SUCCESS;
+}
+
+template <class T>
+int potrf_lower(int64_t n, View<T> A, int* info, cudaStream_t s) {
+    if (!info) return RC_ERR_INVALID_ARGUMENT;
+    if (cudaMemsetAsync(info, 0, sizeof(int), s) != cudaSuccess) return RC_ERR_CUDA;
+    if (n <= 0) return RC_SUCCESS;
+    T* W = static_cast<T*>(workspace(s, (size_t)NB * NB * sizeof(T), 1));
+    if (!W) return RC_ERR_ALLOC;
+    // FP64 panels run on the 128x128 DMMA tile, so one CTA owns every column of a panel
+    // row block and the panel solve can write in place; other types go through a buffer.
+    constexpr bool in_place = std::is_same<T, double>::value;
+    T* tmp = nullptr;
+    if (!in_place) {
+        tmp = static_cast<T*>(workspace(s, (size_t)n * NB * sizeof(T), 2));
+        if (!tmp) return RC_ERR_ALLOC;
+    }
+    RC_TRY(set_smem(potrf_diag<T>, kBlockSmem));
+    const View<const T> Wt = {W, NB, 1};  // inv(L_kk)^T
+    for (int64_t k0 = 0; k0 < n; k0 += NB) {
+        const int sz = (int)((n - k0) < NB ? n - k0 : NB);
+        potrf_diag<T><<<1, 256, kBlockSmem, s>>>(A.sub(k0, k0), sz, k0, W, info);
+        RC_TRY(check_launch());
+        const int64_t rows = n - k0 - sz;
+        if (rows <= 0) break;
+        View<T> P = A.sub(k0 + sz, k0);
+        const View<const T> Pc = {P.p, P.rs, P.cs};
+        if (in_place) {
+            RC_TRY(gemm<T>(rows, sz, sz, T(1), Pc, Wt, T(0), P, kFull, 0, s, info));
+        } else {
+            const View<T> Tv = colmajor(tmp, rows);
+            RC_TRY(gemm<T>(rows, sz, sz, T(1), Pc, Wt, T(0), Tv, kFull, 0, s, info));
+            RC_TRY(copy2d<T, T>(rows, sz, T(1), View<const T>{Tv.p, Tv.rs, Tv.cs}, P, s, info));
+        }
+        RC_TRY(gemm<T>(rows, rows, sz, T(-1), Pc, Pc.t(), T(1), A.sub(k0 + sz, k0 + sz), kLower, 0, s, info));
+    }
+    return RC_SUCCESS;
+}
+
+template int trsm_left<double>(bool, bool, int64_t, int64_t, double, View<const double>, View<double>, int*,
+                               cudaStream_t, const int*);
+template int trsm_left<float>(bool, bool, int64_t, int64_t, float, View<const float>, View<float>, int*,
+                              cudaStream_t, const int*);
+template int potrf_lower<double>(int64_t, View<double>, int*, cudaStream_t);
+template int potrf_lower<float>(int64_t, View<float>, int*, cudaStream_t);
+
+}  // namespace rc
+
+namespace {
+
+template <class T>
+int trsm_abi(int left, int upper, int trans, int unit, size_t m, size_t n, T alpha, const T* A, size_t lda, T* B,
+             size_t ldb, int* d_info, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (d_info && cudaMemsetAsync(d_info, 0, sizeof(int), s) != cudaSuccess) return RC_ERR_CUDA;
+    if (m == 0 || n == 0) return RC_SUCCESS;
+    const size_t na = left ? m : n;
+    if (!A || !B || lda < na || ldb < m) return RC_ERR_INVALID_ARGUMENT;
+    rc::View<const T> a = rc::colmajor(A, (int64_t)lda);
+    bool up = upper != 0;
+    if (trans) { a = a.t(); up = !up; }
+    rc::View<T> b = rc::colmajor(B, (int64_t)ldb);
+    if (left) return rc::trsm_left<T>(up, unit != 0, (int64_t)m, (int64_t)n, alpha, a, b, d_info, s);
+    // B op(A)^-1: solve op(A)^T X^T = alpha B^T on the left.
+    return rc::trsm_left<T>(!up, unit != 0, (int64_t)n, (int64_t)m, alpha, a.t(), b.t(), d_info, s);
+}
+
+template <class T>
+int potrf_abi(int upper, size_t n, T* A, size_t lda, int* d_info, void* stream) {
+    if (!d_info) return RC_ERR_INVALID_ARGUMENT;
+    if (n > 0 && (!A || lda < n)) return RC_ERR_INVALID_ARGUMENT;
+    rc::View<T> a = rc::colmajor(A, (int64_t)lda);
+    if (upper) a = a.t();
+    return rc::potrf_lower<T>((int64_t)n, a, d_info, static_cast<cudaStream_t>(stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+int rc_trsm_f64(int left, int upper, int trans, int unit, size_t m, size_t n, double alpha, const double* A,
+                size_t lda, double* B, size_t ldb, int* d_info, void* stream) {
+    return trsm_abi<double>(left, upper, trans, unit, m, n, alpha, A, lda, B, ldb, d_info, stream);
+}
+int rc_trsm_f32(int left, int upper, int trans, int unit, size_t m, size_t n, float alpha, const float* A,
+                size_t lda, float* B, size_t ldb, int* d_info, void* stream) {
+    return trsm_abi<float>(left, upper, trans, unit, m, n, alpha, A, lda, B, ldb, d_info, stream);
+}
+int rc_potrf_f64(int upper, size_t n, double* A, size_t lda, int* d_info, void* stream) {
+    return potrf_abi<double>(upper, n, A, lda, d_info, stream);
+}
+int rc_potrf_f32(int upper, size_t n, float* A, size_t lda, int* d_info, void* stream) {
+    return potrf_abi<float>(upper, n, A, lda, d_info, stream);
+}
+
+int rc_spd_solve_f64(size_t n, size_t nrhs, const double* A, size_t lda, double* B, size_t ldb, int* d_info,
+                     void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!d_info) return RC_ERR_INVALID_ARGUMENT;
+    if (n == 0) return cudaMemsetAsync(d_info, 0, sizeof(int), s) == cudaSuccess ? RC_SUCCESS : RC_ERR_CUDA;
+    if (!A || lda < n || (nrhs > 0 && (!B || ldb < n))) return RC_ERR_INVALID_ARGUMENT;
+    // The reference copies A into the decomposition's own storage (decompositions.hpp:81-84).
+    double* L = static_cast<double*>(rc::workspace(s, n * n * sizeof(double), 3));
+    if (!L) return RC_ERR_ALLOC;
+    const rc::View<double> Lv = rc::colmajor(L, (int64_t)n);
+    RC_TRY(rc::copy2d<double, double>((int64_t)n, (int64_t)n, 1.0, rc::colmajor(A, (int64_t)lda), Lv, s));
+    RC_TRY(rc::potrf_lower<double>((int64_t)n, Lv, d_info, s));
+    if (nrhs == 0) return RC_SUCCESS;
+    const rc::View<const double> Lc = {L, 1, (int64_t)n};
+    const rc::View<double> Bv = rc::colmajor(B, (int64_t)ldb);
+    RC_TRY(rc::trsm_left<double>(false, false, (int64_t)n, (int64_t)nrhs, 1.0, Lc, Bv, nullptr, s, d_info));
+    return rc::trsm_left<double>(true, false, (int64_t)n, (int64_t)nrhs, 1.0, Lc.t(), Bv, nullptr, s, d_info);
+}
+
+}  // extern "C"

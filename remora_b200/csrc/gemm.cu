@@ -1,0 +1,327 @@
+// Dense GEMM / SYRK for Remora's cuda_tag.
+//
+// Replaces the reference's cuBLAS calls behind kernels::gemm and kernels::syrk
+// (include/remora/hip/cublas_backend.hpp:121-166, :389-431, called from
+// include/remora/kernels/hip/gemm.hpp:46-112 and kernels/hip/syrk.hpp:44-85).
+//
+// Two kernels:
+//  * gemm_dmma_f64: the FP64 tensor-core path (DMMA, mma.sync m16n8k4 f64). 128x128x16
+//    CTA tiles, 8 warps of 64x32, a 3-stage cp.async pipeline. Operand tiles are staged
+//    in shared memory in one canonical layout ([k][m] and [k][n], rows padded by 4
+//    doubles so every fragment load of a half-warp hits 16 distinct 8-byte bank pairs);
+//    the transposition that a K-major operand needs happens in the 8-byte cp.async
+//    scatter, so all four transpose combinations share one inner loop.
+//  * gemm_simt: a generic strided FP32/FP64 kernel (64x64x16 tiles, 4x4 outer products
+//    per thread) for operands with no unit stride and for FP32.
+// Both honour a triangle mask (SYRK writes one triangle; whole tiles outside it exit at
+// once) and an abort word (a failed Cholesky pivot stops the trailing updates).
+#include "gemm.cuh"
+#include <type_traits>
+
+namespace rc {
+namespace {
+
+__device__ __forceinline__ bool aborted(const int* abort) { return abort != nullptr && *(volatile const int*)abort != 0; }
+
+__device__ __forceinline__ bool tile_outside(Mask mask, int64_t off, int64_t m0, int64_t n0, int bm, int bn) {
+    if (mask == kLower) return (m0 + bm - 1) - n0 - off < 0;
+    if (mask == kUpper) return m0 - (n0 + bn - 1) - off > 0;
+    return false;
+}
+
+__device__ __forceinline__ bool in_mask(Mask mask, int64_t off, int64_t i, int64_t j) {
+    if (mask == kLower) return i - j >= off;
+    if (mask == kUpper) return i - j <= off;
+    return true;
+}
+
+// ------------------------------------------------------------------------------------
+// Generic SIMT kernel.
+template <class T>
+__global__ void __launch_bounds__(256) gemm_simt(int64_t m, int64_t n, int64_t k, T alpha, View<const T> A,
+                                                 View<const T> B, T beta, View<T> C, Mask mask, int64_t off,
+                                                 const int* abort) {
+    constexpr int BM = 64, BN = 64, BK = 16;
+    __shared__ T sA[BK][BM + 1];
+    __shared__ T sB[BK][BN + 1];
+    const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
+    if (aborted(abort) || tile_outside(mask, off, m0, n0, BM, BN)) return;
+    const int tid = threadIdx.x;
+    const int tm = tid / 16, tn = tid % 16;  // 16 x 16 threads, 4 x 4 each
+    T acc[4][4] = {};
+    for (int64_t k0 = 0; k0 < k; k0 += BK) {
+        for (int e = tid; e < BM * BK; e += 256) {
+            // A tile: consecutive threads walk the unit-stride direction when there is one.
+            int mm, kk;
+            if (A.rs == 1) { mm = e % BM; kk = e / BM; } else { kk = e % BK; mm = e / BK; }
+            const int64_t gi = m0 + mm, gk = k0 + kk;
+            sA[kk][mm] = (gi < m && gk < k) ? A(gi, gk) : T(0);
+            int nn, kb;
+            if (B.cs == 1) { nn = e % BN; kb = e / BN; } else { kb = e % BK; nn = e / BK; }
+            const int64_t gj = n0 + nn, gk2 = k0 + kb;
+            sB[kb][nn] = (gj < n && gk2 < k) ? B(gk2, gj) : T(0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            T a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) a[r] = sA[kk][tm + 16 * r];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) b[c] = sB[kk][tn + 16 * c];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int64_t i = m0 + tm + 16 * r;
+        if (i >= m) continue;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int64_t j = n0 + tn + 16 * c;
+            if (j >= n || !in_mask(mask, off, i, j)) continue;
+            T v = alpha * acc[r][c];
+            if (beta != T(0)) v = fma(beta, C(i, j), v);
+            C(i, j) = v;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// FP64 DMMA kernel.
+constexpr int DM = 128, DN = 128, DK = 16, DSTAGES = 3, DPAD = 4;
+constexpr int DLDA = DM + DPAD, DLDB = DN + DPAD;
+constexpr size_t kDmmaSmem = (size_t)DSTAGES * DK * (DLDA + DLDB) * sizeof(double);
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int bytes = pred ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1, double b0) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// A_KMAJOR: A(i, k) is contiguous along k (A.cs == 1), else along i (A.rs == 1).
+// B_KMAJOR: B(k, j) is contiguous along k (B.rs == 1), else along j (B.cs == 1).
+template <bool A_KMAJOR, bool B_KMAJOR>
+__device__ __forceinline__ void dmma_load_tile(double* sA, double* sB, const View<const double>& A,
+                                               const View<const double>& B, int64_t m, int64_t n, int64_t k,
+                                               int64_t m0, int64_t n0, int64_t k0, int tid) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        int mm, kk;
+        if (A_KMAJOR) { kk = tid % 16; mm = tid / 16 + 16 * r; } else { mm = tid % 128; kk = tid / 128 + 2 * r; }
+        const int64_t gi = m0 + mm, gk = k0 + kk;
+        const bool ok = gi < m && gk < k;
+        cp_async8(sA + kk * DLDA + mm, ok ? &A(gi, gk) : A.p, ok);
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        int nn, kk;
+        if (B_KMAJOR) { kk = tid % 16; nn = tid / 16 + 16 * r; } else { nn = tid % 128; kk = tid / 128 + 2 * r; }
+        const int64_t gj = n0 + nn, gk = k0 + kk;
+        const bool ok = gj < n && gk < k;
+        cp_async8(sB + kk * DLDB + nn, ok ? &B(gk, gj) : B.p, ok);
+    }
+}
+
+template <bool A_KMAJOR, bool B_KMAJOR>
+__global__ void __launch_bounds__(256, 1) gemm_dmma_f64(int64_t m, int64_t n, int64_t k, double alpha,
+                                                         View<const double> A, View<const double> B, double beta,
+                                                         View<double> C, Mask mask, int64_t off,
+                                                         const int* abort) {
+    extern __shared__ __align__(16) double dsmem[];
+    double* sA = dsmem;
+    double* sB = dsmem + DSTAGES * DK * DLDA;
+    const int64_t m0 = (int64_t)blockIdx.y * DM, n0 = (int64_t)blockIdx.x * DN;
+    if (aborted(abort) || tile_outside(mask, off, m0, n0, DM, DN)) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;
+    double acc[4][4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
+
+    const int KT = (int)((k + DK - 1) / DK);
+#pragma unroll
+    for (int s = 0; s < DSTAGES - 1; ++s) {
+        if (s < KT)
+            dmma_load_tile<A_KMAJOR, B_KMAJOR>(sA + s * DK * DLDA, sB + s * DK * DLDB, A, B, m, n, k, m0, n0,
+                                               (int64_t)s * DK, tid);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < KT; ++kt) {
+        cp_async_wait<DSTAGES - 2>();
+        __syncthreads();
+        const int pf = kt + DSTAGES - 1;
+        if (pf < KT) {
+            const int st = pf % DSTAGES;
+            dmma_load_tile<A_KMAJOR, B_KMAJOR>(sA + st * DK * DLDA, sB + st * DK * DLDB, A, B, m, n, k, m0, n0,
+                                               (int64_t)pf * DK, tid);
+        }
+        cp_async_commit();
+        const double* a_s = sA + (kt % DSTAGES) * DK * DLDA;
+        const double* b_s = sB + (kt % DSTAGES) * DK * DLDB;
+#pragma unroll
+        for (int ks = 0; ks < DK; ks += 4) {
+            double af[4][2], bf[4];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi) {
+                af[mi][0] = a_s[(ks + t) * DLDA + wm + mi * 16 + g];
+                af[mi][1] = a_s[(ks + t) * DLDA + wm + mi * 16 + g + 8];
+            }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) bf[ni] = b_s[(ks + t) * DLDB + wn + ni * 8 + g];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+        }
+    }
+    cp_async_wait<0>();
+    // Epilogue: element (g, 2t + c) and (g + 8, 2t + c) of each 16x8 accumulator tile.
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t i = m0 + wm + mi * 16 + g + 8 * h;
+            if (i >= m) continue;
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const int64_t j = n0 + wn + ni * 8 + 2 * t + c;
+                    if (j >= n || !in_mask(mask, off, i, j)) continue;
+                    double v = alpha * acc[mi][ni][2 * h + c];
+                    if (beta != 0.0) v = fma(beta, C(i, j), v);
+                    C(i, j) = v;
+                }
+        }
+}
+
+template <bool AK, bool BK>
+int launch_dmma(int64_t m, int64_t n, int64_t k, double alpha, View<const double> A, View<const double> B,
+                double beta, View<double> C, Mask mask, int64_t off, cudaStream_t s, const int* abort) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(gemm_dmma_f64<AK, BK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kDmmaSmem) != cudaSuccess)
+            return RC_ERR_CUDA;
+        attr_set = true;
+    }
+    dim3 grid(ceil_div(n, DN), ceil_div(m, DM));
+    gemm_dmma_f64<AK, BK><<<grid, 256, kDmmaSmem, s>>>(m, n, k, alpha, A, B, beta, C, mask, off, abort);
+    return check_launch();
+}
+
+// Scale (beta != 1) the masked part of C when k == 0 or alpha == 0.
+template <class T>
+__global__ void scale_masked(int64_t m, int64_t n, T beta, View<T> C, Mask mask, int64_t off, const int* abort) {
+    if (aborted(abort)) return;
+    for (int64_t j = blockIdx.y; j < n; j += gridDim.y)
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+            if (in_mask(mask, off, i, j)) C(i, j) = beta == T(0) ? T(0) : beta * C(i, j);
+}
+
+}  // namespace
+
+template <class T>
+int gemm(int64_t m, int64_t n, int64_t k, T alpha, View<const T> A, View<const T> B, T beta, View<T> C, Mask mask,
+         int64_t off, cudaStream_t s, const int* abort) {
+    if (m <= 0 || n <= 0) return RC_SUCCESS;
+    if (k <= 0 || alpha == T(0)) {
+        if (beta == T(1)) return RC_SUCCESS;
+        dim3 grid(ceil_div(m, 256) < 1024u ? ceil_div(m, 256) : 1024u, n < 65535 ? (unsigned)n : 65535u);
+        scale_masked<T><<<grid, 256, 0, s>>>(m, n, beta, C, mask, off, abort);
+        return check_launch();
+    }
+    if constexpr (std::is_same<T, double>::value) {
+        const bool a_k = A.cs == 1, a_m = A.rs == 1, b_k = B.rs == 1, b_n = B.cs == 1;
+        if ((a_k || a_m) && (b_k || b_n)) {
+            if (a_k && b_k) return launch_dmma<true, true>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
+            if (a_k) return launch_dmma<true, false>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
+            if (b_k) return launch_dmma<false, true>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
+            return launch_dmma<false, false>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
+        }
+    }
+    dim3 grid(ceil_div(n, 64), ceil_div(m, 64));
+    gemm_simt<T><<<grid, 256, 0, s>>>(m, n, k, alpha, A, B, beta, C, mask, off, abort);
+    return check_launch();
+}
+
+template int gemm<double>(int64_t, int64_t, int64_t, double, View<const double>, View<const double>, double,
+                          View<double>, Mask, int64_t, cudaStream_t, const int*);
+template int gemm<float>(int64_t, int64_t, int64_t, float, View<const float>, View<const float>, float,
+                         View<float>, Mask, int64_t, cudaStream_t, const int*);
+
+}  // namespace rc
+
+namespace {
+
+template <class T>
+int gemm_abi(int transA, int transB, size_t m, size_t n, size_t k, T alpha, const T* A, size_t lda, const T* B,
+             size_t ldb, T beta, T* C, size_t ldc, void* stream) {
+    if (m == 0 || n == 0) return RC_SUCCESS;
+    if (!C || ldc < m) return RC_ERR_INVALID_ARGUMENT;
+    if (k > 0) {
+        if (!A || !B) return RC_ERR_INVALID_ARGUMENT;
+        if (lda < (transA ? k : m) || ldb < (transB ? n : k)) return RC_ERR_INVALID_ARGUMENT;
+    }
+    rc::View<const T> a = rc::colmajor(A, (int64_t)lda);
+    rc::View<const T> b = rc::colmajor(B, (int64_t)ldb);
+    if (transA) a = a.t();
+    if (transB) b = b.t();
+    return rc::gemm<T>((int64_t)m, (int64_t)n, (int64_t)k, alpha, a, b, beta, rc::colmajor(C, (int64_t)ldc),
+                       rc::kFull, 0, static_cast<cudaStream_t>(stream));
+}
+
+template <class T>
+int syrk_abi(int upper, int trans, size_t n, size_t k, T alpha, const T* A, size_t lda, T beta, T* C, size_t ldc,
+             void* stream) {
+    if (n == 0) return RC_SUCCESS;
+    if (!C || ldc < n) return RC_ERR_INVALID_ARGUMENT;
+    if (k > 0 && (!A || lda < (trans ? k : n))) return RC_ERR_INVALID_ARGUMENT;
+    rc::View<const T> a = rc::colmajor(A, (int64_t)lda);
+    if (trans) a = a.t();  // op(A) = A^T, n x k
+    return rc::gemm<T>((int64_t)n, (int64_t)n, (int64_t)k, alpha, a, a.t(), beta, rc::colmajor(C, (int64_t)ldc),
+                       upper ? rc::kUpper : rc::kLower, 0, static_cast<cudaStream_t>(stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+int rc_gemm_f64(int transA, int transB, size_t m, size_t n, size_t k, double alpha, const double* A, size_t lda,
+                const double* B, size_t ldb, double beta, double* C, size_t ldc, void* stream) {
+    return gemm_abi<double>(transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, stream);
+}
+int rc_gemm_f32(int transA, int transB, size_t m, size_t n, size_t k, float alpha, const float* A, size_t lda,
+                const float* B, size_t ldb, float beta, float* C, size_t ldc, void* stream) {
+    return gemm_abi<float>(transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, stream);
+}
+int rc_syrk_f64(int upper, int trans, size_t n, size_t k, double alpha, const double* A, size_t lda, double beta,
+                double* C, size_t ldc, void* stream) {
+    return syrk_abi<double>(upper, trans, n, k, alpha, A, lda, beta, C, ldc, stream);
+}
+int rc_syrk_f32(int upper, int trans, size_t n, size_t k, float alpha, const float* A, size_t lda, float beta,
+                float* C, size_t ldc, void* stream) {
+    return syrk_abi<float>(upper, trans, n, k, alpha, A, lda, beta, C, ldc, stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,162 @@
+"""Python view of the Remora kernel API on ``cuda`` tensors, through the C-ABI.
+
+The functions mirror the reference's kernel entry points and their semantics:
+
+=====================================  ==================================================
+``gemm(A, B, C, alpha)``               ``kernels::gemm`` -- C += alpha * A * B
+                                       (include/remora/kernels/gemm.hpp:85-106)
+``syrk(A, C, alpha, upper)``           ``kernels::syrk<Upper>`` -- one triangle of C
+                                       += alpha * A * A^T (kernels/syrk.hpp:55-67)
+``trsm(A, B, upper, unit, left)``      ``kernels::trsm<Tri, Side>`` (kernels/trsm.hpp:55-65)
+``potrf(A, upper) -> int``             ``kernels::potrf<Tri>`` (kernels/potrf.hpp:56-62),
+                                       0 or the global 1-based failing pivot
+``cholesky_solve(A, B)``               ``cholesky_decomposition(A).solve(B, left())``
+                                       (decompositions.hpp:81-105)
+``generate_normal/uniform/discrete``   ``kernels::generate_*`` for a device matrix
+                                       (kernels/hip/random.hpp:262-323)
+=====================================  ==================================================
+
+Matrices are 2-D torch tensors on a CUDA device in row-major or column-major storage
+(strided sub-matrices allowed); orientation is read from the strides, as Remora reads it
+from the ``orientation`` type. Everything runs on the current torch stream.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import torch
+
+from ._lib import call, key_array
+
+_FP = {torch.float64: "f64", torch.float32: "f32"}
+
+
+def _stream() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t: torch.Tensor) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def layout(X: torch.Tensor) -> tuple[int, int]:
+    """(trans, ld) with X = op_trans(M), M column-major with leading dimension ld."""
+    if X.dim() != 2:
+        raise ValueError("expected a matrix")
+    r, c = X.shape
+    s0, s1 = X.stride()
+    if s0 == 1 and (c <= 1 or s1 >= max(r, 1)):
+        return 0, max(s1 if c > 1 else r, 1)
+    if s1 == 1 and (r <= 1 or s0 >= max(c, 1)):
+        return 1, max(s0 if r > 1 else c, 1)
+    raise ValueError(f"matrix with strides {X.stride()} is neither row- nor column-major")
+
+
+def is_row_major(X: torch.Tensor) -> bool:
+    return layout(X)[0] == 1
+
+
+def _sfx(*ts: torch.Tensor) -> str:
+    dt = ts[0].dtype
+    if any(t.dtype != dt for t in ts) or dt not in _FP:
+        raise TypeError("arguments must share one element type, float32 or float64")
+    return _FP[dt]
+
+
+def gemm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, alpha: float = 1.0, beta: float = 1.0,
+         tf32: bool = False) -> None:
+    """C <- alpha * A @ B + beta * C (beta = 1 is the reference's kernels::gemm)."""
+    sfx = "tf32" if tf32 else _sfx(A, B, C)
+    m, n = C.shape
+    k = A.shape[1]
+    if A.shape[0] != m or B.shape != (k, n):
+        raise ValueError("gemm: shape mismatch")
+    ta, lda = layout(A)
+    tb, ldb = layout(B)
+    tc, ldc = layout(C)
+    if tc == 0:
+        call(f"rc_gemm_{sfx}", ta, tb, m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb, beta, _ptr(C), ldc, _stream())
+    else:  # C^T = B^T A^T, column-major
+        call(f"rc_gemm_{sfx}", 1 - tb, 1 - ta, n, m, k, alpha, _ptr(B), ldb, _ptr(A), lda, beta, _ptr(C), ldc,
+             _stream())
+
+
+def syrk(A: torch.Tensor, C: torch.Tensor, alpha: float = 1.0, upper: bool = False, beta: float = 1.0) -> None:
+    """One triangle of C <- alpha * A @ A^T + beta * C; the other triangle is untouched."""
+    sfx = _sfx(A, C)
+    n, k = A.shape
+    if C.shape != (n, n):
+        raise ValueError("syrk: shape mismatch")
+    ta, lda = layout(A)
+    tc, ldc = layout(C)
+    up = bool(upper) != bool(tc)  # a row-major C is the transpose of a column-major one
+    call(f"rc_syrk_{sfx}", int(up), ta, n, k, alpha, _ptr(A), lda, beta, _ptr(C), ldc, _stream())
+
+
+def trsm(A: torch.Tensor, B: torch.Tensor, upper: bool = False, unit: bool = False, left: bool = True,
+         alpha: float = 1.0, info: torch.Tensor | None = None) -> None:
+    """B <- alpha * A^-1 B (left) or alpha * B A^-1 (right), A the named triangle."""
+    sfx = _sfx(A, B)
+    m, n = B.shape
+    ta, lda = layout(A)
+    tb, ldb = layout(B)
+    up_stored = bool(upper) != bool(ta)
+    if tb == 0:
+        side, trans, mm, nn = left, ta, m, n
+    else:  # B^T is column-major: X^T = B^T A^-T on the other side
+        side, trans, mm, nn = not left, 1 - ta, n, m
+    call(f"rc_trsm_{sfx}", int(side), int(up_stored), trans, int(unit), mm, nn, alpha, _ptr(A), lda, _ptr(B), ldb,
+         _ptr(info) if info is not None else None, _stream())
+
+
+def potrf(A: torch.Tensor, upper: bool = False, info: torch.Tensor | None = None, sync: bool = True):
+    """In-place Cholesky; returns 0 or the global 1-based failing pivot (sync=True)."""
+    sfx = _sfx(A)
+    n = A.shape[0]
+    ta, lda = layout(A)
+    if info is None:
+        info = torch.zeros(1, dtype=torch.int32, device=A.device)
+    call(f"rc_potrf_{sfx}", int(bool(upper) != bool(ta)), n, _ptr(A), lda, _ptr(info), _stream())
+    return int(info.item()) if sync else info
+
+
+def cholesky_solve(A: torch.Tensor, B: torch.Tensor, info: torch.Tensor | None = None) -> int:
+    """B <- A^-1 B for SPD A (FP64; A's lower triangle read, A unchanged)."""
+    if A.dtype != torch.float64 or B.dtype != torch.float64:
+        raise TypeError("cholesky_solve is FP64")
+    n = A.shape[0]
+    ta, lda = layout(A)  # A symmetric: a row-major A is the same matrix read column-major
+    tb, ldb = layout(B)
+    if tb != 0:
+        raise ValueError("cholesky_solve: B must be column-major")
+    if info is None:
+        info = torch.zeros(1, dtype=torch.int32, device=A.device)
+    call("rc_spd_solve_f64", n, B.shape[1], _ptr(A), lda, _ptr(B), ldb, _ptr(info), _stream())
+    return int(info.item())
+
+
+def _fill(kind: str, X: torch.Tensor, key, a, b) -> None:
+    rows, cols = X.shape
+    t, ld = layout(X)
+    call(f"rc_rng_{kind}", key_array(key), rows, cols, _ptr(X), ld, t, a, b, _stream())
+
+
+def generate_normal(X: torch.Tensor, key, mean: float = 0.0, variance: float = 1.0) -> None:
+    """Normal fill; the reference passes sqrt(variance) as the scale (random.hpp:270, :280)."""
+    _fill("normal_f32", X, key, mean, math.sqrt(variance))
+
+
+def generate_uniform(X: torch.Tensor, key, low: float = 0.0, high: float = 1.0) -> None:
+    _fill("uniform_f32", X, key, low, high)
+
+
+def generate_discrete(X: torch.Tensor, key, low: int, high: int) -> None:
+    _fill("discrete_i32" if X.dtype == torch.int32 else "discrete_f32", X, key, int(low), int(high))
+
+
+def generate_bits(X: torch.Tensor, key) -> None:
+    """Raw Threefry words (uint32 stored in an int32 tensor)."""
+    rows, cols = X.shape
+    t, ld = layout(X)
+    call("rc_rng_bits_u32", key_array(key), rows, cols, _ptr(X), ld, t, _stream())

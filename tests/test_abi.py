@@ -1,0 +1,54 @@
+"""The C-ABI library loads without a GPU and exports every entry point its header declares."""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import remora_b200
+from remora_b200 import _lib
+
+HEADERS = sorted((Path(__file__).resolve().parents[1] / "include").glob("*.h"))
+
+
+def declared_symbols() -> set[str]:
+    names = set()
+    for h in HEADERS:
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(rc_\w+)\s*\(", text))
+    return names
+
+
+def test_library_loads_and_exports_header_symbols():
+    lib = remora_b200.lib()
+    names = declared_symbols()
+    assert len(names) >= 20
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header():
+    assert declared_symbols() <= set(_lib.SIGNATURES)
+
+
+def test_host_only_entry_points():
+    lib = remora_b200.lib()
+    assert lib.rc_version() >= 100
+    assert lib.rc_error_string(0) == b"success"
+    assert b"invalid" in lib.rc_error_string(1)
+
+
+def test_argument_checks_need_no_device():
+    """Size/leading-dimension checks return RC_ERR_INVALID_ARGUMENT before any CUDA call."""
+    lib = remora_b200.lib()
+    fake = ctypes.c_void_p(16)
+    # lda < m
+    assert lib.rc_gemm_f64(0, 0, 10, 10, 10, 1.0, fake, 5, fake, 10, 0.0, fake, 10, None) == 1
+    # potrf without a status word
+    assert lib.rc_potrf_f64(0, 10, fake, 10, None, None) == 1
+    # discrete range reversed
+    key = _lib.key_array([1, 2, 3, 4])
+    assert lib.rc_rng_discrete_i32(key, 4, 4, fake, 4, 1, 5, 2, None) == 1
+    # empty problems are no-ops
+    assert lib.rc_gemm_f32(0, 0, 0, 5, 5, 1.0, None, 1, None, 1, 0.0, None, 1, None) == 0
