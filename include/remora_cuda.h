@@ -39,6 +39,16 @@ int rc_version(void);
 const char* rc_error_string(int status);
 /* Free every cached workspace of the current device (synchronises the device). */
 int rc_release_workspaces(void);
+/* Failure detection. Every device-side wait (mbarrier phases of the tensor-core
+ * pipelines, the batched solver's cross-CTA flags) is bounded by a wall-clock limit
+ * (default 2 s); a wait that runs out records RC_ERR_TIMEOUT in a per-device error word
+ * and its kernel returns, leaving the context usable. rc_device_status synchronises the
+ * stream and returns (then clears) that word. rc_selftest_wait_timeout launches one
+ * bounded wait on a barrier that nothing completes, to exercise that path. These have
+ * no reference counterpart (the reference checks no launch, hip/exception.hpp:41-63). */
+int rc_set_wait_limit_ns(uint64_t ns);
+int rc_device_status(void* stream);
+int rc_selftest_wait_timeout(uint64_t limit_ns, void* stream);
 
 /* ---------------------------------------------------------------------------------
  * Counter-based RNG fills of a rows x cols float/int matrix (Threefry-4x32, 12 rounds).
@@ -65,13 +75,24 @@ int rc_rng_discrete_i32(const uint32_t key[4], size_t rows, size_t cols, int32_t
  * C <- alpha * op(A) * op(B) + beta * C, C m x n, op(A) m x k, op(B) k x n.
  * Replaces kernels::gemm for hip_tag (include/remora/kernels/hip/gemm.hpp:46-112 ->
  * include/remora/hip/cublas_backend.hpp:121-166). beta == 0 does not read C.
- * rc_gemm_f64: FP64 on the DMMA tensor path; rc_gemm_f32: FP32-accurate. */
+ * rc_gemm_f64: FP64 on the DMMA tensor path; rc_gemm_f32: FP32-accurate (large shapes on the
+ * tensor cores with a 3-term TF32 split, small ones on FP32 FMA). */
 int rc_gemm_f64(int transA, int transB, size_t m, size_t n, size_t k, double alpha,
                 const double* A, size_t lda, const double* B, size_t ldb, double beta,
                 double* C, size_t ldc, void* stream);
 int rc_gemm_f32(int transA, int transB, size_t m, size_t n, size_t k, float alpha,
                 const float* A, size_t lda, const float* B, size_t ldb, float beta,
                 float* C, size_t ldc, void* stream);
+/* Reduced-precision FP32 GEMMs on the tcgen05 tensor cores with FP32 accumulation:
+ * rc_gemm_tf32 truncates the operands to TF32 (10 mantissa bits), rc_gemm_bf16 rounds
+ * them to BF16. No reference counterpart (the reference's FP32 gemm is cuBLAS SGEMM);
+ * they are the precisions of the mixed-precision solve's trailing updates. */
+int rc_gemm_tf32(int transA, int transB, size_t m, size_t n, size_t k, float alpha,
+                 const float* A, size_t lda, const float* B, size_t ldb, float beta,
+                 float* C, size_t ldc, void* stream);
+int rc_gemm_bf16(int transA, int transB, size_t m, size_t n, size_t k, float alpha,
+                 const float* A, size_t lda, const float* B, size_t ldb, float beta,
+                 float* C, size_t ldc, void* stream);
 
 /* C_tri <- alpha * op(A) * op(A)^T + beta * C_tri on the upper or lower triangle of the
  * n x n matrix C; op(A) is n x k (trans = 0: A is n x k; trans = 1: A is k x n). The

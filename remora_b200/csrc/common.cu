@@ -56,11 +56,39 @@ void* workspace(cudaStream_t stream, size_t bytes, int slot) {
 
 int* scratch_info(cudaStream_t stream) { return static_cast<int*>(workspace(stream, 256, 15)); }
 
+namespace {
+std::map<int, int*> g_error_words;
+uint64_t g_wait_limit_ns = 2000000000ull;
+}  // namespace
+
+int* error_word() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lock(g_mutex);
+    int*& w = g_error_words[dev];
+    if (!w) {
+        if (cudaMalloc(&w, sizeof(int)) != cudaSuccess || cudaMemset(w, 0, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            w = nullptr;
+        }
+    }
+    return w;
+}
+
+uint64_t wait_limit_ns() { return g_wait_limit_ns; }
+void set_wait_limit_ns(uint64_t ns) { g_wait_limit_ns = ns; }
+
 }  // namespace rc
 
 extern "C" {
 
 int rc_version(void) { return 100; }
+
+int rc_set_wait_limit_ns(uint64_t ns) {
+    if (ns == 0) return RC_ERR_INVALID_ARGUMENT;
+    rc::set_wait_limit_ns(ns);
+    return RC_SUCCESS;
+}
 
 const char* rc_error_string(int status) {
     switch (status) {

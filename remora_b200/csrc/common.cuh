@@ -45,6 +45,15 @@ void* workspace(cudaStream_t stream, size_t bytes, int slot = 0);
 // Device int used as a per-call status word when the caller passes none.
 int* scratch_info(cudaStream_t stream);
 
+// The library's device error word of the current device (zero-initialised once): kernels
+// whose bounded waits run out write RC_ERR_TIMEOUT there; rc_device_status reads and
+// clears it.
+int* error_word();
+
+// Wall-clock limit of every bounded device-side wait, in nanoseconds (default 2 s).
+uint64_t wait_limit_ns();
+void set_wait_limit_ns(uint64_t ns);
+
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
 
 }  // namespace rc

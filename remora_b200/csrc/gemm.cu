@@ -16,6 +16,7 @@
 // Both honour a triangle mask (SYRK writes one triangle; whole tiles outside it exit at
 // once) and an abort word (a failed Cholesky pivot stops the trailing updates).
 #include "gemm.cuh"
+#include "tc_gemm.cuh"
 #include <type_traits>
 
 namespace rc {
@@ -258,6 +259,13 @@ int gemm(int64_t m, int64_t n, int64_t k, T alpha, View<const T> A, View<const T
             if (a_k) return launch_dmma<true, false>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
             if (b_k) return launch_dmma<false, true>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
             return launch_dmma<false, false>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
+        }
+    }
+    if constexpr (std::is_same<T, float>::value) {
+        // Large FP32 products run on the tensor cores with the 3-term TF32 split.
+        if (m >= 128 && n >= 128 && k >= 64) {
+            const int r = gemm_tf32(m, n, k, alpha, A, B, beta, C, mask, off, true, s, abort);
+            if (r != RC_ERR_NOT_SUPPORTED) return r;
         }
     }
     dim3 grid(ceil_div(n, 64), ceil_div(m, 64));

@@ -1,0 +1,18 @@
+// Internal entry points of the tcgen05 GEMM.
+#pragma once
+#include "gemm.cuh"
+
+namespace rc {
+
+// D = alpha * A * B^T + beta * C with A (m x k) and B (n x k) K-major buffers (row r at
+// ptr + r * ld) of FP32 (TF32 products) or BF16; 16-byte aligned pointers and rows.
+// bn: tile width (128 or 256; 0 picks one). Returns RC_ERR_NOT_SUPPORTED on layouts the
+// TMA cannot describe.
+int gemm_tc_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, const void* A, int64_t lda,
+                   const void* B, int64_t ldb, float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s,
+                   const int* abort = nullptr, int bn = 0);
+
+// Copy rows x K of X into a K-major buffer (row stride ldd), as FP32 or rounded to BF16.
+int pack_kmajor(int64_t rows, int64_t K, View<const float> X, void* dst, int64_t ldd, bool bf16, cudaStream_t s);
+
+}  // namespace rc

@@ -1,0 +1,87 @@
+"""tcgen05 tensor-core GEMMs (TF32 and BF16 operands, FP32 accumulation) through the
+C-ABI, and the bounded-wait failure path.
+
+The TF32/BF16 products are compared against an FP64 product of the SAME reduced-precision
+operands (TF32: low 13 mantissa bits cleared; BF16: rounded to nearest even), so the bar
+(relative Frobenius <= 2e-6) tests the kernel's data movement and accumulation exactly;
+any layout or descriptor error shows as O(1)."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from remora_b200 import _lib, ops
+from helpers import to_host
+
+pytestmark = pytest.mark.gpu
+TC_TOL = 2e-6
+
+
+def _tf32(x: torch.Tensor) -> torch.Tensor:
+    return (x.view(torch.int32) & ~0x1FFF).view(torch.float32)
+
+
+def _rel(a: torch.Tensor, b: torch.Tensor) -> float:
+    return ((a.double() - b.double()).norm() / b.double().norm()).item()
+
+
+SHAPES = [(128, 128, 32), (1, 1, 1), (7, 300, 13), (256, 256, 256), (300, 500, 1000), (1000, 129, 77),
+          (2048, 1024, 4096)]
+
+
+@pytest.mark.parametrize("m,n,k", SHAPES)
+@pytest.mark.parametrize("ta,tb", [(1, 0), (0, 0), (1, 1), (0, 1)])
+def test_gemm_tf32(cuda, m, n, k, ta, tb):
+    g = torch.Generator(device="cuda").manual_seed(m + 3 * n + 7 * k)
+    A = torch.rand((m, k), generator=g, device="cuda") * 2 - 1
+    B = torch.rand((k, n), generator=g, device="cuda") * 2 - 1
+    C = torch.rand((m, n), generator=g, device="cuda") * 2 - 1
+    Ad = A.t().contiguous().t() if not ta else A.contiguous()
+    Bd = B.t().contiguous().t() if not tb else B.contiguous()
+    ref = 0.5 * (_tf32(A).double() @ _tf32(B).double()) - 1.5 * C.double()
+    Cd = C.t().contiguous().t()
+    ops.gemm(Ad, Bd, Cd, alpha=0.5, beta=-1.5, tf32=True)
+    assert _rel(Cd, ref) <= TC_TOL
+
+
+@pytest.mark.parametrize("m,n,k", SHAPES)
+def test_gemm_bf16(cuda, m, n, k):
+    g = torch.Generator(device="cuda").manual_seed(m * 5 + n + k)
+    A = torch.rand((m, k), generator=g, device="cuda") * 2 - 1
+    B = torch.rand((k, n), generator=g, device="cuda") * 2 - 1
+    ref = A.bfloat16().double() @ B.bfloat16().double()
+    C = torch.zeros((n, m), device="cuda").t()
+    _lib.call("rc_gemm_bf16", 0, 0, m, n, k, 1.0, ctypes.c_void_p(A.t().contiguous().data_ptr()), m,
+              ctypes.c_void_p(B.t().contiguous().data_ptr()), k, 0.0, ctypes.c_void_p(C.data_ptr()), m,
+              ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert _rel(C, ref) <= TC_TOL
+
+
+def test_fp32_gemm_uses_tf32_split_accuracy(cuda):
+    """rc_gemm_f32 on a large shape (3-term TF32 split) stays FP32-accurate."""
+    m = n = k = 2048
+    g = torch.Generator(device="cuda").manual_seed(9)
+    A = torch.rand((m, k), generator=g, device="cuda") * 2 - 1
+    B = torch.rand((k, n), generator=g, device="cuda") * 2 - 1
+    C = torch.zeros((m, n), device="cuda")
+    ops.gemm(A, B, C, alpha=1.0, beta=0.0)
+    ref = A.double() @ B.double()
+    assert _rel(C, ref) <= 1e-6
+
+
+def test_bounded_wait_times_out_and_context_survives(cuda):
+    lib = _lib.lib()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert lib.rc_device_status(stream) == 0
+    assert lib.rc_selftest_wait_timeout(50_000_000, stream) == 0  # a 50 ms wait that nothing completes
+    assert lib.rc_device_status(stream) == 5  # RC_ERR_TIMEOUT, read and cleared
+    assert lib.rc_device_status(stream) == 0
+    # the context is still usable
+    A = torch.ones((256, 256), device="cuda")
+    C = torch.zeros((256, 256), device="cuda")
+    ops.gemm(A, A, C, alpha=1.0, beta=0.0, tf32=True)
+    assert torch.all(C == 256.0)
+    assert lib.rc_device_status(stream) == 0
