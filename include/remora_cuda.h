@@ -75,8 +75,7 @@ int rc_rng_discrete_i32(const uint32_t key[4], size_t rows, size_t cols, int32_t
  * C <- alpha * op(A) * op(B) + beta * C, C m x n, op(A) m x k, op(B) k x n.
  * Replaces kernels::gemm for hip_tag (include/remora/kernels/hip/gemm.hpp:46-112 ->
  * include/remora/hip/cublas_backend.hpp:121-166). beta == 0 does not read C.
- * rc_gemm_f64: FP64 on the DMMA tensor path; rc_gemm_f32: FP32-accurate (large shapes on the
- * tensor cores with a 3-term TF32 split, small ones on FP32 FMA). */
+ * rc_gemm_f64: FP64 on the DMMA tensor path; rc_gemm_f32: FP32 FMA (IEEE FP32 accuracy). */
 int rc_gemm_f64(int transA, int transB, size_t m, size_t n, size_t k, double alpha,
                 const double* A, size_t lda, const double* B, size_t ldb, double beta,
                 double* C, size_t ldc, void* stream);

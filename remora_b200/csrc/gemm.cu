@@ -261,13 +261,6 @@ int gemm(int64_t m, int64_t n, int64_t k, T alpha, View<const T> A, View<const T
             return launch_dmma<false, false>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
         }
     }
-    if constexpr (std::is_same<T, float>::value) {
-        // Large FP32 products run on the tensor cores with the 3-term TF32 split.
-        if (m >= 128 && n >= 128 && k >= 64) {
-            const int r = gemm_tf32(m, n, k, alpha, A, B, beta, C, mask, off, true, s, abort);
-            if (r != RC_ERR_NOT_SUPPORTED) return r;
-        }
-    }
     dim3 grid(ceil_div(n, 64), ceil_div(m, 64));
     gemm_simt<T><<<grid, 256, 0, s>>>(m, n, k, alpha, A, B, beta, C, mask, off, abort);
     return check_launch();

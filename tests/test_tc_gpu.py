@@ -3,7 +3,7 @@ C-ABI, and the bounded-wait failure path.
 
 The TF32/BF16 products are compared against an FP64 product of the SAME reduced-precision
 operands (TF32: low 13 mantissa bits cleared; BF16: rounded to nearest even), so the bar
-(relative Frobenius <= 2e-6) tests the kernel's data movement and accumulation exactly;
+(relative Frobenius <= 1e-5, the FP32 accumulation error of K <= 4096 terms) tests the kernel's data movement and accumulation exactly;
 any layout or descriptor error shows as O(1)."""
 from __future__ import annotations
 
@@ -17,7 +17,7 @@ from remora_b200 import _lib, ops
 from helpers import to_host
 
 pytestmark = pytest.mark.gpu
-TC_TOL = 2e-6
+TC_TOL = 1e-5
 
 
 def _tf32(x: torch.Tensor) -> torch.Tensor:
@@ -54,22 +54,27 @@ def test_gemm_bf16(cuda, m, n, k):
     B = torch.rand((k, n), generator=g, device="cuda") * 2 - 1
     ref = A.bfloat16().double() @ B.bfloat16().double()
     C = torch.zeros((n, m), device="cuda").t()
-    _lib.call("rc_gemm_bf16", 0, 0, m, n, k, 1.0, ctypes.c_void_p(A.t().contiguous().data_ptr()), m,
-              ctypes.c_void_p(B.t().contiguous().data_ptr()), k, 0.0, ctypes.c_void_p(C.data_ptr()), m,
+    Acm, Bcm = A.t().contiguous(), B.t().contiguous()  # column-major copies, kept alive across the call
+    _lib.call("rc_gemm_bf16", 0, 0, m, n, k, 1.0, ctypes.c_void_p(Acm.data_ptr()), m,
+              ctypes.c_void_p(Bcm.data_ptr()), k, 0.0, ctypes.c_void_p(C.data_ptr()), m,
               ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
     assert _rel(C, ref) <= TC_TOL
 
 
-def test_fp32_gemm_uses_tf32_split_accuracy(cuda):
-    """rc_gemm_f32 on a large shape (3-term TF32 split) stays FP32-accurate."""
+def test_fp32_and_tf32_accuracy(cuda):
+    """rc_gemm_f32 (FP32 FMA) is FP32-accurate against FP64; rc_gemm_tf32 carries the
+    TF32 operand truncation (~2^-11 per operand), so its error sits between 1e-5 and 2e-3."""
     m = n = k = 2048
     g = torch.Generator(device="cuda").manual_seed(9)
     A = torch.rand((m, k), generator=g, device="cuda") * 2 - 1
     B = torch.rand((k, n), generator=g, device="cuda") * 2 - 1
-    C = torch.zeros((m, n), device="cuda")
-    ops.gemm(A, B, C, alpha=1.0, beta=0.0)
     ref = A.double() @ B.double()
+    C = torch.zeros((m, n), device="cuda")
+    ops.gemm(A, B, C, alpha=1.0, beta=0.0)  # FP32 FMA
     assert _rel(C, ref) <= 1e-6
+    ops.gemm(A, B, C, alpha=1.0, beta=0.0, tf32=True)
+    assert 1e-5 < _rel(C, ref) < 2e-3
 
 
 def test_bounded_wait_times_out_and_context_survives(cuda):
