@@ -132,6 +132,43 @@ int rc_spd_solve_f64(size_t n, size_t nrhs, const double* A, size_t lda, double*
                      int* d_info, void* stream);
 
 /* ---------------------------------------------------------------------------------
+ * Mixed-precision refined SPD solve (extension; no reference counterpart -- the reference
+ * solves SPD systems only in the working precision, decompositions.hpp:81-105).
+ * X = A^-1 B for a symmetric positive definite A given in FULL (both triangles), FP64:
+ *  - factor S A S + theta I (S = diag(A)^-1/2, theta = shift_factor * u_f) in FP32 storage
+ *    with FP64 diagonal blocks and TF32 or BF16 tensor-core trailing updates (FP32
+ *    accumulation);
+ *  - refine in FP64 (FP64 residuals and products) by preconditioned conjugate gradients
+ *    with that factor, per right-hand side, until the normwise backward error
+ *    ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol on every column.
+ * The call synchronises the stream (convergence is decided on the host). Returns
+ * RC_ERR_NOT_CONVERGED when max_iter is reached first; d_info receives the failing pivot
+ * when the low-precision factorisation breaks down (then X is not written). */
+enum { RC_PREC_TF32 = 0, RC_PREC_BF16 = 1 };
+typedef struct {
+    double tol;          /* backward-error target (<= 0: 1e-15) */
+    int max_iter;        /* CG iterations allowed in total (< 0: 100) */
+    int outer;           /* outer panel width, a multiple of 128 (<= 0: 1024) */
+    double shift_factor; /* theta = shift_factor * u_f (< 0: 1) */
+} rc_mixed_options;
+typedef struct {
+    int iterations;        /* preconditioned CG iterations */
+    int residuals;         /* true FP64 residual evaluations */
+    int converged;         /* 1 when every column met tol */
+    double backward_error; /* max over columns, from the last true residual */
+    double factor_ms;      /* device time of the low-precision factorisation */
+    double refine_ms;      /* device + host time of the refinement */
+    double shift;          /* theta actually used */
+} rc_refine_info;
+int rc_spd_solve_mixed(int precision, size_t n, size_t nrhs, const double* A, size_t lda,
+                       const double* B, size_t ldb, double* X, size_t ldx,
+                       const rc_mixed_options* options, int* d_info, rc_refine_info* info,
+                       void* stream);
+/* Device workspace the solve caches for these sizes, in bytes. */
+int rc_spd_solve_mixed_workspace(int precision, size_t n, size_t nrhs,
+                                 const rc_mixed_options* options, size_t* bytes);
+
+/* ---------------------------------------------------------------------------------
  * Assignment support for the containers (include/remora/kernels/hip/matrix_assign.hpp:
  * 38-200, include/remora/hip/dense.hpp:39-51, hip/buffer.hpp:105-125).
  * rc_copy2d_*: B <- alpha * op(A) (A m x n if !trans, n x m if trans; B m x n).

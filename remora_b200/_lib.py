@@ -13,6 +13,17 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libremora_cuda.so"
 
 RC_SUCCESS = 0
+RC_PREC_TF32 = 0
+RC_PREC_BF16 = 1
+
+
+class MixedOptions(ctypes.Structure):
+    _fields_ = [("tol", c_double), ("max_iter", c_int), ("outer", c_int), ("shift_factor", c_double)]
+
+
+class RefineInfo(ctypes.Structure):
+    _fields_ = [("iterations", c_int), ("residuals", c_int), ("converged", c_int), ("backward_error", c_double),
+                ("factor_ms", c_double), ("refine_ms", c_double), ("shift", c_double)]
 STATUS_NAMES = {0: "RC_SUCCESS", 1: "RC_ERR_INVALID_ARGUMENT", 2: "RC_ERR_CUDA", 3: "RC_ERR_ALLOC",
                 4: "RC_ERR_NOT_SUPPORTED", 5: "RC_ERR_TIMEOUT", 6: "RC_ERR_NOT_CONVERGED"}
 
@@ -45,6 +56,8 @@ SIGNATURES: dict[str, list] = {
     "rc_potrf_f64": [_I, _Z, _P, _Z, _P, _P],
     "rc_potrf_f32": [_I, _Z, _P, _Z, _P, _P],
     "rc_spd_solve_f64": [_Z, _Z, _P, _Z, _P, _Z, _P, _P],
+    "rc_spd_solve_mixed": [_I, _Z, _Z, _P, _Z, _P, _Z, _P, _Z, _P, _P, _P, _P],
+    "rc_spd_solve_mixed_workspace": [_I, _Z, _Z, _P, _P],
     "rc_copy2d_f64": [_I, _Z, _Z, c_double, _P, _Z, _P, _Z, _P],
     "rc_copy2d_f32": [_I, _Z, _Z, c_float, _P, _Z, _P, _Z, _P],
     "rc_fill_f64": [_Z, _Z, c_double, _P, _Z, _P],

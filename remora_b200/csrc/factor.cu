@@ -54,11 +54,12 @@ __device__ void invert_lower_inplace(double* S, bool unit) {
     __syncthreads();
 }
 
-// Store the inverse (lower, zero above the diagonal) as a column-major NB x NB block.
+// Store the inverse (lower, zero above the diagonal) as an NB x NB block, column-major or
+// (row_major) row-major.
 template <class T>
-__device__ void store_block(const double* S, T* W) {
+__device__ void store_block(const double* S, T* W, bool row_major = false) {
     for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
-        const int i = e % NB, j = e / NB;
+        const int i = row_major ? e / NB : e % NB, j = row_major ? e % NB : e / NB;
         W[e] = j <= i ? (T)S[i * SLD + j] : T(0);
     }
 }
@@ -88,7 +89,8 @@ __global__ void __launch_bounds__(NB) trtri_blocks(int64_t m, View<const T> L, b
 // Factor the sz x sz lower diagonal block (A already offset to it) in FP64 shared
 // memory, write L back, and store inv(L) into W. g0 = global index of the block.
 template <class T>
-__global__ void __launch_bounds__(256) potrf_diag(View<T> A, int sz, int64_t g0, T* W, int* info) {
+__global__ void __launch_bounds__(256) potrf_diag(View<T> A, int sz, int64_t g0, T* W, int* info,
+                                                  bool w_row_major) {
     extern __shared__ double S[];
     if (aborted(info)) return;
     const int tid = threadIdx.x;
@@ -120,7 +122,7 @@ __global__ void __launch_bounds__(256) potrf_diag(View<T> A, int sz, int64_t g0,
     }
     __syncthreads();
     invert_lower_inplace(S, false);
-    store_block<T>(S, W);
+    store_block<T>(S, W, w_row_major);
 }
 
 template <class K>
@@ -182,7 +184,7 @@ int potrf_lower(int64_t n, View<T> A, int* info, cudaStream_t s) {
     const View<const T> Wt = {W, NB, 1};  // inv(L_kk)^T
     for (int64_t k0 = 0; k0 < n; k0 += NB) {
         const int sz = (int)((n - k0) < NB ? n - k0 : NB);
-        potrf_diag<T><<<1, 256, kBlockSmem, s>>>(A.sub(k0, k0), sz, k0, W, info);
+        potrf_diag<T><<<1, 256, kBlockSmem, s>>>(A.sub(k0, k0), sz, k0, W, info, false);
         RC_TRY(check_launch());
         const int64_t rows = n - k0 - sz;
         if (rows <= 0) break;
@@ -200,6 +202,40 @@ int potrf_lower(int64_t n, View<T> A, int* info, cudaStream_t s) {
     return RC_SUCCESS;
 }
 
+template <class T>
+int potrf_diag_block(View<T> A, int sz, int64_t g0, T* W, bool w_row_major, int* info, cudaStream_t s) {
+    RC_TRY(set_smem(potrf_diag<T>, kBlockSmem));
+    potrf_diag<T><<<1, 256, kBlockSmem, s>>>(A, sz, g0, W, info, w_row_major);
+    return check_launch();
+}
+
+template <class T>
+int trsm_preinv(bool trans, int64_t m, int64_t n, View<const T> L, const T* Winv, View<T> B, T* tmp, cudaStream_t s) {
+    if (m <= 0 || n <= 0) return RC_SUCCESS;
+    const int64_t nblk = (m + NB - 1) / NB;
+    const View<T> Tv = colmajor(tmp, (int64_t)NB);
+    const View<const T> Tc = {tmp, 1, (int64_t)NB};
+    for (int64_t step = 0; step < nblk; ++step) {
+        const int64_t b = trans ? nblk - 1 - step : step;
+        const int64_t r0 = b * NB, sz = (m - r0 < NB) ? m - r0 : NB;
+        const View<const T> X = {Winv + (size_t)b * NB * NB, NB, 1};
+        View<T> Bb = B.sub(r0, 0);
+        const View<const T> Bc = {Bb.p, Bb.rs, Bb.cs};
+        RC_TRY(gemm<T>(sz, n, sz, T(1), trans ? X.t() : X, Bc, T(0), Tv, kFull, 0, s));
+        RC_TRY(copy2d<T, T>(sz, n, T(1), Tc, Bb, s));
+        if (!trans && r0 + sz < m)
+            RC_TRY(gemm<T>(m - r0 - sz, n, sz, T(-1), L.sub(r0 + sz, r0), Bc, T(1), B.sub(r0 + sz, 0), kFull, 0, s));
+        if (trans && r0 > 0) RC_TRY(gemm<T>(r0, n, sz, T(-1), L.sub(r0, 0).t(), Bc, T(1), B, kFull, 0, s));
+    }
+    return RC_SUCCESS;
+}
+
+template int potrf_diag_block<float>(View<float>, int, int64_t, float*, bool, int*, cudaStream_t);
+template int potrf_diag_block<double>(View<double>, int, int64_t, double*, bool, int*, cudaStream_t);
+template int trsm_preinv<float>(bool, int64_t, int64_t, View<const float>, const float*, View<float>, float*,
+                                cudaStream_t);
+template int trsm_preinv<double>(bool, int64_t, int64_t, View<const double>, const double*, View<double>, double*,
+                                 cudaStream_t);
 template int trsm_left<double>(bool, bool, int64_t, int64_t, double, View<const double>, View<double>, int*,
                                cudaStream_t, const int*);
 template int trsm_left<float>(bool, bool, int64_t, int64_t, float, View<const float>, View<float>, int*,

@@ -32,4 +32,16 @@ int trsm_left(bool upper, bool unit, int64_t m, int64_t n, T alpha, View<const T
 template <class T>
 int potrf_lower(int64_t n, View<T> A, int* info, cudaStream_t s);
 
+// Factor one sz x sz (sz <= kNB) lower diagonal block of A (view offset to the block)
+// in FP64 shared memory, write L back and store inv(L) as a kNB x kNB block into W
+// (row-major when w_row_major). g0 is the block's global index for the pivot status.
+template <class T>
+int potrf_diag_block(View<T> A, int sz, int64_t g0, T* W, bool w_row_major, int* info, cudaStream_t s);
+
+// Blocked triangular solve with precomputed inverses of the kNB diagonal blocks of the
+// lower-triangular L (row-major blocks, as potrf_diag_block stores them):
+// trans = false: B <- L^-1 B; trans = true: B <- L^-T B. tmp holds kNB x n elements.
+template <class T>
+int trsm_preinv(bool trans, int64_t m, int64_t n, View<const T> L, const T* Winv, View<T> B, T* tmp, cudaStream_t s);
+
 }  // namespace rc

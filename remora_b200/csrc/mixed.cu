@@ -1,0 +1,459 @@
+// Mixed-precision refined SPD solve: an extension on top of the reference's
+// cholesky_decomposition + solve (include/remora/decompositions.hpp:81-105), with no
+// reference counterpart of its own.
+//
+//  1. Equilibrate and shift: W = fl32(S A S) + theta I with S = diag(A)^(-1/2), stored as
+//     an FP32 row-major working copy (so every panel row is contiguous: the K-major layout
+//     the tcgen05 GEMM reads through TMA). theta = shift_factor * u_f (u_f = 2^-11 for TF32,
+//     2^-8 for BF16) keeps the low-precision factorisation from breaking down on
+//     ill-conditioned A (Higham & Pranesh 2021, diagonal scaling + shift).
+//  2. Factor W = L L^T, blocked right-looking: outer panels of `outer` columns, inner
+//     128-column blocks whose diagonal block is factored (and inverted) in FP64 shared
+//     memory; the panel below is solved with that inverse on the TF32 tensor cores; the
+//     updates inside the panel and the trailing update run on the tcgen05 tensor cores in
+//     TF32 or BF16 with FP32 accumulation (BF16 operands are packed per panel).
+//  3. Refine in FP64: x0 = M^-1 b with M = S^-1 L L^T S^-1, then preconditioned conjugate
+//     gradients on A (FP64 residuals and matrix products on the DMMA path, FP64 vectors,
+//     the FP32 factor as preconditioner), one independent CG recurrence per right-hand
+//     side, stopped per column when the normwise backward error
+//         ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
+//     of the TRUE residual is at most tol (CG-based iterative refinement for SPD systems:
+//     Higham & Pranesh 2021; GMRES-IR: Carson & Higham 2017/2018).
+#include <cmath>
+#include <vector>
+
+#include "assign.cuh"
+#include "factor.cuh"
+#include "gemm.cuh"
+#include "mixed.cuh"
+#include "tc_gemm.cuh"
+
+namespace rc {
+namespace {
+
+// s_i = 1 / sqrt(A_ii) (1 where A_ii <= 0, which the factorisation then reports).
+__global__ void diag_scale_kernel(int64_t n, View<const double> A, double* s) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double d = A(i, i);
+        s[i] = d > 0.0 ? 1.0 / sqrt(d) : 1.0;
+    }
+}
+
+// W[i * ldw + j] = fl32(s_i A(i, j) s_j) (+ theta on the diagonal) for the lower triangle
+// (j <= i), through a 32 x 33 tile so reads of column-major A and writes of row-major W
+// are both coalesced.
+__global__ void __launch_bounds__(256) scale_to_f32_kernel(int64_t n, View<const double> A, const double* s,
+                                                           double theta, float* W, int64_t ldw) {
+    __shared__ float tile[32][33];
+    const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
+    if (j0 > i0 + 31) return;  // tile strictly above the diagonal
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < 32; r += 8) {  // read: consecutive threads walk i (A's unit stride)
+        const int64_t i = i0 + tx, j = j0 + r;
+        float v = 0.f;
+        if (i < n && j < n && j <= i) v = (float)(s[i] * A(i, j) * s[j] + (i == j ? theta : 0.0));
+        tile[r][tx] = v;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {  // write: consecutive threads walk j (W's unit stride)
+        const int64_t i = i0 + r, j = j0 + tx;
+        if (i < n && j < n && j <= i) W[i * ldw + j] = tile[tx][r];
+    }
+}
+
+// ||A||_inf of the symmetric A as the largest column sum of |A| (coalesced column walks).
+__global__ void __launch_bounds__(256) col_abs_sum_kernel(int64_t n, View<const double> A, double* out) {
+    __shared__ double red[256];
+    for (int64_t j = blockIdx.x; j < n; j += gridDim.x) {
+        double acc = 0.0;
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) acc += fabs(A(i, j));
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = 128; w > 0; w >>= 1) {
+            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[j] = red[0];
+        __syncthreads();
+    }
+}
+
+// Per-column reductions of n x c column-major FP64 blocks: mode 0 max|u|, mode 1 u.v.
+__global__ void __launch_bounds__(256) col_reduce_kernel(int64_t n, int64_t c, const double* U, int64_t ldu,
+                                                         const double* V, int64_t ldv, int mode, double* out) {
+    __shared__ double red[256];
+    for (int64_t j = blockIdx.x; j < c; j += gridDim.x) {
+        double acc = 0.0;
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const double u = U[i + j * ldu];
+            acc = mode == 0 ? fmax(acc, fabs(u)) : fma(u, V[i + j * ldv], acc);
+        }
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = 128; w > 0; w >>= 1) {
+            if (threadIdx.x < w)
+                red[threadIdx.x] = mode == 0 ? fmax(red[threadIdx.x], red[threadIdx.x + w])
+                                             : red[threadIdx.x] + red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[j] = red[0];
+        __syncthreads();
+    }
+}
+
+// Y[:, j] += a[j] * X[:, j] (sign folded into a).
+__global__ void col_axpy_kernel(int64_t n, int64_t c, const double* a, const double* X, int64_t ldx, double* Y,
+                                int64_t ldy) {
+    for (int64_t j = blockIdx.y; j < c; j += gridDim.y) {
+        const double aj = a[j];
+        if (aj == 0.0) continue;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            Y[i + j * ldy] = fma(aj, X[i + j * ldx], Y[i + j * ldy]);
+    }
+}
+
+// P[:, j] = Z[:, j] + b[j] * P[:, j] for active columns (b[j] >= 0); inactive: untouched.
+__global__ void col_xpby_kernel(int64_t n, int64_t c, const double* b, const double* Z, int64_t ldz, double* P,
+                                int64_t ldp) {
+    for (int64_t j = blockIdx.y; j < c; j += gridDim.y) {
+        const double bj = b[j];
+        if (bj < 0.0) continue;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            P[i + j * ldp] = fma(bj, P[i + j * ldp], Z[i + j * ldz]);
+    }
+}
+
+// T = fl32(s .* R) (row scaling) and back: Z = s .* T.
+__global__ void to_f32_scaled_kernel(int64_t n, int64_t c, const double* s, const double* R, int64_t ldr, float* T) {
+    for (int64_t j = blockIdx.y; j < c; j += gridDim.y)
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            T[i + j * n] = (float)(s[i] * R[i + j * ldr]);
+}
+__global__ void from_f32_scaled_kernel(int64_t n, int64_t c, const double* s, const float* T, double* Z, int64_t ldz) {
+    for (int64_t j = blockIdx.y; j < c; j += gridDim.y)
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            Z[i + j * ldz] = s[i] * (double)T[i + j * n];
+}
+
+dim3 vec_grid(int64_t n, int64_t c) {
+    return dim3(ceil_div(n, 256) < 256u ? ceil_div(n, 256) : 256u, c < 65535 ? (unsigned)c : 65535u);
+}
+
+struct Buf {
+    char* base;
+    size_t used = 0;
+    template <class T>
+    T* take(size_t count) {
+        T* p = reinterpret_cast<T*>(base + used);
+        used += (count * sizeof(T) + 255) & ~size_t(255);
+        return p;
+    }
+};
+
+}  // namespace
+
+int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* bytes) {
+    const int64_t ldw = (n + 31) / 32 * 32;
+    const int64_t nblk = (n + kNB - 1) / kNB;
+    const int64_t ow = outer > 0 ? outer : 1024;
+    size_t b = 0;
+    auto add = [&](size_t x) { b += (x + 255) & ~size_t(255); };
+    add((size_t)n * ldw * sizeof(float));               // W
+    add((size_t)nblk * kNB * kNB * sizeof(float));      // diagonal-block inverses
+    if (prec == RC_PREC_BF16) add((size_t)n * ((ow + 63) / 64 * 64) * 2);  // BF16 panel
+    add((size_t)n * sizeof(double));                    // s
+    add((size_t)n * sizeof(double));                    // column sums
+    for (int i = 0; i < 4; ++i) add((size_t)n * nrhs * sizeof(double));  // R, Z, P, Q
+    add((size_t)n * nrhs * sizeof(float));              // FP32 right-hand side of the preconditioner
+    add((size_t)kNB * nrhs * sizeof(float));            // TRSM tile buffer
+    add((size_t)8 * nrhs * sizeof(double));             // per-column scalars
+    *bytes = b;
+    return RC_SUCCESS;
+}
+
+namespace {
+
+struct Mixed {
+    int64_t n, nrhs, ldw, nblk;
+    int prec;
+    cudaStream_t s;
+    const double* A;
+    int64_t lda;
+    float* W;
+    float* Winv;
+    void* Pb;
+    int64_t ldpb;
+    double* sc;
+    double* colsum;
+    double *R, *Z, *P, *Q;
+    float* T32;
+    float* tmp;
+    double* dev_scalars;  // 8 x nrhs
+    View<const double> Av() const { return {A, 1, lda}; }
+    View<float> Wv() const { return {W, ldw, 1}; }
+
+    int factor(int outer, int* info) {
+        const View<float> Wm = Wv();
+        for (int64_t k0 = 0; k0 < n; k0 += outer) {
+            const int64_t w = (n - k0 < outer) ? n - k0 : outer;
+            for (int64_t j0 = k0; j0 < k0 + w; j0 += kNB) {
+                const int jb = (int)((k0 + w - j0) < kNB ? k0 + w - j0 : kNB);
+                float* Wb = Winv + (size_t)(j0 / kNB) * kNB * kNB;
+                RC_TRY(potrf_diag_block<float>(Wm.sub(j0, j0), jb, j0, Wb, true, info, s));
+                const int64_t rows = n - j0 - jb;
+                if (rows <= 0) continue;
+                View<float> Pj = Wm.sub(j0 + jb, j0);
+                // Panel solve in place: P <- P inv(L_jj)^T (TF32 tensor cores, one column tile).
+                RC_TRY(gemm_tc_kmajor(false, rows, jb, jb, 1.f, Pj.p, ldw, Wb, kNB, 0.f, Pj, kFull, 0, s, info, 128));
+                const int64_t cw = k0 + w - (j0 + jb);
+                if (cw <= 0) continue;
+                const void* op = Pj.p;
+                int64_t ldo = ldw;
+                if (prec == RC_PREC_BF16) {
+                    RC_TRY(pack_kmajor(rows, jb, View<const float>{Pj.p, Pj.rs, Pj.cs}, Pb, ldpb, true, s));
+                    op = Pb;
+                    ldo = ldpb;
+                }
+                RC_TRY(gemm_tc_kmajor(prec == RC_PREC_BF16, rows, cw, jb, -1.f, op, ldo, op, ldo, 1.f,
+                                      Wm.sub(j0 + jb, j0 + jb), kLower, 0, s, info));
+            }
+            const int64_t rows = n - k0 - w;
+            if (rows <= 0) continue;
+            View<float> Pk = Wm.sub(k0 + w, k0);
+            const void* op = Pk.p;
+            int64_t ldo = ldw;
+            if (prec == RC_PREC_BF16) {
+                RC_TRY(pack_kmajor(rows, w, View<const float>{Pk.p, Pk.rs, Pk.cs}, Pb, ldpb, true, s));
+                op = Pb;
+                ldo = ldpb;
+            }
+            RC_TRY(gemm_tc_kmajor(prec == RC_PREC_BF16, rows, rows, w, -1.f, op, ldo, op, ldo, 1.f,
+                                  Wm.sub(k0 + w, k0 + w), kLower, 0, s, info));
+        }
+        return RC_SUCCESS;
+    }
+
+    // Zout = M^-1 Rin = S L^-T L^-1 S Rin (FP64 in/out, FP32 triangular solves).
+    int precond(const double* Rin, int64_t ldr, double* Zout, int64_t ldz) {
+        const dim3 g = vec_grid(n, nrhs);
+        to_f32_scaled_kernel<<<g, 256, 0, s>>>(n, nrhs, sc, Rin, ldr, T32);
+        RC_TRY(check_launch());
+        const View<const float> L = {W, ldw, 1};
+        const View<float> Tv = colmajor(T32, n);
+        RC_TRY(trsm_preinv<float>(false, n, nrhs, L, Winv, Tv, tmp, s));
+        RC_TRY(trsm_preinv<float>(true, n, nrhs, L, Winv, Tv, tmp, s));
+        from_f32_scaled_kernel<<<g, 256, 0, s>>>(n, nrhs, sc, T32, Zout, ldz);
+        return check_launch();
+    }
+
+    // Rout = B - A X (FP64, DMMA).
+    int residual(const double* B, int64_t ldb, const double* X, int64_t ldx, double* Rout) {
+        RC_TRY(copy2d<double, double>(n, nrhs, 1.0, View<const double>{B, 1, ldb}, colmajor(Rout, n), s));
+        return gemm<double>(n, nrhs, n, -1.0, Av(), View<const double>{X, 1, ldx}, 1.0, colmajor(Rout, n), kFull, 0,
+                            s);
+    }
+
+    int col_reduce(const double* U, int64_t ldu, const double* V, int64_t ldv, int mode, std::vector<double>& out,
+                   double* dst) {
+        col_reduce_kernel<<<(unsigned)(nrhs < 1024 ? nrhs : 1024), 256, 0, s>>>(n, nrhs, U, ldu, V, ldv, mode, dst);
+        RC_TRY(check_launch());
+        out.resize(nrhs);
+        if (cudaMemcpyAsync(out.data(), dst, nrhs * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return RC_ERR_CUDA;
+        return RC_SUCCESS;
+    }
+
+    int upload(const std::vector<double>& v, double* dst) {
+        return cudaMemcpyAsync(dst, v.data(), nrhs * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess
+                   ? RC_SUCCESS
+                   : RC_ERR_CUDA;
+    }
+};
+
+}  // namespace
+
+int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t lda, const double* B, int64_t ldb,
+                    double* X, int64_t ldx, const rc_mixed_options* opt, int* d_info, rc_refine_info* out,
+                    cudaStream_t s) {
+    rc_mixed_options o = {};
+    o.tol = 1e-15;
+    o.max_iter = 100;
+    o.outer = 1024;
+    o.shift_factor = -1.0;
+    if (opt) o = *opt;
+    if (o.outer <= 0 || o.outer % kNB) o.outer = 1024;
+    if (o.tol <= 0) o.tol = 1e-15;
+    if (o.max_iter < 0) o.max_iter = 100;
+    const double uf = prec == RC_PREC_BF16 ? std::ldexp(1.0, -8) : std::ldexp(1.0, -11);
+    const double theta = (o.shift_factor >= 0.0 ? o.shift_factor : 1.0) * uf;
+
+    size_t bytes = 0;
+    mixed_workspace_bytes(n, nrhs, prec, o.outer, &bytes);
+    char* base = static_cast<char*>(workspace(s, bytes, 6));
+    if (!base) return RC_ERR_ALLOC;
+    Buf buf{base};
+    Mixed M;
+    M.n = n; M.nrhs = nrhs; M.prec = prec; M.s = s; M.A = A; M.lda = lda;
+    M.ldw = (n + 31) / 32 * 32;
+    M.nblk = (n + kNB - 1) / kNB;
+    M.W = buf.take<float>((size_t)n * M.ldw);
+    M.Winv = buf.take<float>((size_t)M.nblk * kNB * kNB);
+    M.ldpb = (o.outer + 63) / 64 * 64;
+    M.Pb = prec == RC_PREC_BF16 ? static_cast<void*>(buf.take<uint16_t>((size_t)n * M.ldpb)) : nullptr;
+    M.sc = buf.take<double>(n);
+    M.colsum = buf.take<double>(n);
+    M.R = buf.take<double>((size_t)n * nrhs);
+    M.Z = buf.take<double>((size_t)n * nrhs);
+    M.P = buf.take<double>((size_t)n * nrhs);
+    M.Q = buf.take<double>((size_t)n * nrhs);
+    M.T32 = buf.take<float>((size_t)n * nrhs);
+    M.tmp = buf.take<float>((size_t)kNB * nrhs);
+    M.dev_scalars = buf.take<double>((size_t)8 * nrhs);
+
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
+    cudaEventRecord(e0, s);
+    if (cudaMemsetAsync(d_info, 0, sizeof(int), s) != cudaSuccess) return RC_ERR_CUDA;
+    const View<const double> Av = M.Av();
+    diag_scale_kernel<<<ceil_div(n, 256) < 1024u ? ceil_div(n, 256) : 1024u, 256, 0, s>>>(n, Av, M.sc);
+    RC_TRY(check_launch());
+    scale_to_f32_kernel<<<dim3(ceil_div(n, 32), ceil_div(n, 32)), 256, 0, s>>>(n, Av, M.sc, theta, M.W, M.ldw);
+    RC_TRY(check_launch());
+    RC_TRY(M.factor(o.outer, d_info));
+    cudaEventRecord(e1, s);
+    int h_info = 0;
+    if (cudaMemcpyAsync(&h_info, d_info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return RC_ERR_CUDA;
+    rc_refine_info info = {};
+    if (h_info != 0) {
+        if (out) *out = info;
+        return RC_SUCCESS;  // d_info reports the failing pivot of the low-precision factor
+    }
+
+    // ||A||_inf, ||b||_inf per column.
+    col_abs_sum_kernel<<<(unsigned)(n < 4096 ? n : 4096), 256, 0, s>>>(n, Av, M.colsum);
+    RC_TRY(check_launch());
+    std::vector<double> tmpv;
+    {
+        // max over the n column sums: reuse the column reduction with c = 1 on an n x 1 block
+        col_reduce_kernel<<<1, 256, 0, s>>>(n, 1, M.colsum, n, nullptr, 0, 0, M.dev_scalars);
+        RC_TRY(check_launch());
+    }
+    double normA = 0.0;
+    if (cudaMemcpyAsync(&normA, M.dev_scalars, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return RC_ERR_CUDA;
+    std::vector<double> normB, normX, normR, rz, pq, alpha(nrhs), beta(nrhs);
+    RC_TRY(M.col_reduce(B, ldb, nullptr, 0, 0, normB, M.dev_scalars));
+
+    // x0 = M^-1 b
+    RC_TRY(M.precond(B, ldb, X, ldx));
+    std::vector<char> done(nrhs, 0);
+    int iters = 0, residuals = 0;
+    double worst = 0.0;
+    bool restart = true;
+    double* const Rm = M.R;
+    const int64_t ldm = n;
+    while (true) {
+        if (restart) {
+            RC_TRY(M.residual(B, ldb, X, ldx, Rm));
+            ++residuals;
+            RC_TRY(M.col_reduce(Rm, ldm, nullptr, 0, 0, normR, M.dev_scalars));
+            RC_TRY(M.col_reduce(X, ldx, nullptr, 0, 0, normX, M.dev_scalars + nrhs));
+            worst = 0.0;
+            for (int64_t j = 0; j < nrhs; ++j) {
+                const double eta = normR[j] / (normA * normX[j] + normB[j]);
+                done[j] = !(eta > o.tol);
+                if (std::isfinite(eta)) worst = std::max(worst, eta);
+                else worst = INFINITY;
+            }
+            bool all = true;
+            for (char d : done) all = all && d;
+            if (all || iters >= o.max_iter) break;
+            // (re)start CG from the true residual: Z = M^-1 R, P = Z, rz = R.Z
+            RC_TRY(M.precond(Rm, ldm, M.Z, ldm));
+            RC_TRY(copy2d<double, double>(n, nrhs, 1.0, View<const double>{M.Z, 1, ldm}, colmajor(M.P, ldm), s));
+            RC_TRY(M.col_reduce(Rm, ldm, M.Z, ldm, 1, rz, M.dev_scalars));
+            restart = false;
+        }
+        // Q = A P; alpha = rz / (P.Q) on the active columns.
+        RC_TRY(gemm<double>(n, nrhs, n, 1.0, Av, View<const double>{M.P, 1, ldm}, 0.0, colmajor(M.Q, ldm), kFull, 0,
+                            s));
+        RC_TRY(M.col_reduce(M.P, ldm, M.Q, ldm, 1, pq, M.dev_scalars));
+        for (int64_t j = 0; j < nrhs; ++j) alpha[j] = (done[j] || pq[j] <= 0.0) ? 0.0 : rz[j] / pq[j];
+        RC_TRY(M.upload(alpha, M.dev_scalars + 2 * nrhs));
+        const dim3 g = vec_grid(n, nrhs);
+        col_axpy_kernel<<<g, 256, 0, s>>>(n, nrhs, M.dev_scalars + 2 * nrhs, M.P, ldm, X, ldx);
+        for (int64_t j = 0; j < nrhs; ++j) alpha[j] = -alpha[j];
+        RC_TRY(M.upload(alpha, M.dev_scalars + 3 * nrhs));
+        col_axpy_kernel<<<g, 256, 0, s>>>(n, nrhs, M.dev_scalars + 3 * nrhs, M.Q, ldm, Rm, ldm);
+        RC_TRY(check_launch());
+        ++iters;
+        // Convergence estimate from the recurrence residual; confirm with a true residual.
+        RC_TRY(M.col_reduce(Rm, ldm, nullptr, 0, 0, normR, M.dev_scalars));
+        RC_TRY(M.col_reduce(X, ldx, nullptr, 0, 0, normX, M.dev_scalars + nrhs));
+        bool all = true;
+        for (int64_t j = 0; j < nrhs; ++j) {
+            if (done[j]) continue;
+            const double eta = normR[j] / (normA * normX[j] + normB[j]);
+            if (!(eta > 0.5 * o.tol)) done[j] = 1;
+            all = all && done[j];
+        }
+        if (all || iters >= o.max_iter) {
+            restart = true;  // verify with the true residual (and restart CG where it fails)
+            continue;
+        }
+        // Z = M^-1 R; beta = rz_new / rz; P = Z + beta P
+        RC_TRY(M.precond(Rm, ldm, M.Z, ldm));
+        std::vector<double> rz_new;
+        RC_TRY(M.col_reduce(Rm, ldm, M.Z, ldm, 1, rz_new, M.dev_scalars));
+        for (int64_t j = 0; j < nrhs; ++j) {
+            beta[j] = done[j] ? -1.0 : (rz[j] != 0.0 ? rz_new[j] / rz[j] : 0.0);
+            rz[j] = rz_new[j];
+        }
+        RC_TRY(M.upload(beta, M.dev_scalars + 4 * nrhs));
+        col_xpby_kernel<<<g, 256, 0, s>>>(n, nrhs, M.dev_scalars + 4 * nrhs, M.Z, ldm, M.P, ldm);
+        RC_TRY(check_launch());
+    }
+    cudaEventRecord(e2, s);
+    cudaEventSynchronize(e2);
+    float t_f = 0.f, t_r = 0.f;
+    cudaEventElapsedTime(&t_f, e0, e1);
+    cudaEventElapsedTime(&t_r, e1, e2);
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+    info.iterations = iters;
+    info.residuals = residuals;
+    info.backward_error = worst;
+    info.converged = worst <= o.tol ? 1 : 0;
+    info.factor_ms = t_f;
+    info.refine_ms = t_r;
+    info.shift = theta;
+    if (out) *out = info;
+    return info.converged ? RC_SUCCESS : RC_ERR_NOT_CONVERGED;
+}
+
+}  // namespace rc
+
+extern "C" {
+
+int rc_spd_solve_mixed(int precision, size_t n, size_t nrhs, const double* A, size_t lda, const double* B, size_t ldb,
+                       double* X, size_t ldx, const rc_mixed_options* options, int* d_info, rc_refine_info* info,
+                       void* stream) {
+    if (precision != RC_PREC_TF32 && precision != RC_PREC_BF16) return RC_ERR_INVALID_ARGUMENT;
+    if (!d_info) return RC_ERR_INVALID_ARGUMENT;
+    if (n == 0 || nrhs == 0) return RC_SUCCESS;
+    if (!A || !B || !X || lda < n || ldb < n || ldx < n) return RC_ERR_INVALID_ARGUMENT;
+    if (n > (size_t)INT32_MAX) return RC_ERR_NOT_SUPPORTED;
+    return rc::spd_solve_mixed(precision, (int64_t)n, (int64_t)nrhs, A, (int64_t)lda, B, (int64_t)ldb, X, (int64_t)ldx,
+                               options, d_info, info, static_cast<cudaStream_t>(stream));
+}
+
+int rc_spd_solve_mixed_workspace(int precision, size_t n, size_t nrhs, const rc_mixed_options* options,
+                                 size_t* bytes) {
+    if (!bytes) return RC_ERR_INVALID_ARGUMENT;
+    return rc::mixed_workspace_bytes((int64_t)n, (int64_t)nrhs, precision, options ? options->outer : 0, bytes);
+}
+
+}  // extern "C"

@@ -160,3 +160,32 @@ def generate_bits(X: torch.Tensor, key) -> None:
     rows, cols = X.shape
     t, ld = layout(X)
     call("rc_rng_bits_u32", key_array(key), rows, cols, _ptr(X), ld, t, _stream())
+
+
+def spd_solve_mixed(A: torch.Tensor, B: torch.Tensor, precision: str = "tf32", tol: float = 1e-15,
+                    max_iter: int = 100, outer: int = 1024, shift_factor: float = -1.0,
+                    X: torch.Tensor | None = None):
+    """Mixed-precision refined SPD solve (FP64 in/out; A full symmetric, column-major).
+
+    Returns (X, info dict, status) -- status 0 on convergence, 6 (RC_ERR_NOT_CONVERGED) when
+    max_iter ran out; info["pivot"] is the failing pivot of a low-precision breakdown."""
+    from ._lib import RC_PREC_BF16, RC_PREC_TF32, MixedOptions, RefineInfo, lib
+    if A.dtype != torch.float64 or B.dtype != torch.float64:
+        raise TypeError("spd_solve_mixed takes FP64 matrices")
+    n = A.shape[0]
+    ta, lda = layout(A)
+    tb, ldb = layout(B)
+    if tb != 0:
+        raise ValueError("B must be column-major")
+    if X is None:
+        X = torch.empty((B.shape[1], n), dtype=torch.float64, device=B.device).t()
+    tx, ldx = layout(X)
+    prec = {"tf32": RC_PREC_TF32, "bf16": RC_PREC_BF16}[precision]
+    opts = MixedOptions(tol, max_iter, outer, shift_factor)
+    info = RefineInfo()
+    d_info = torch.zeros(1, dtype=torch.int32, device=A.device)
+    status = lib().rc_spd_solve_mixed(prec, n, B.shape[1], _ptr(A), lda, _ptr(B), ldb, _ptr(X), ldx,
+                                      ctypes.byref(opts), _ptr(d_info), ctypes.byref(info), _stream())
+    out = {f: getattr(info, f) for f, _ in RefineInfo._fields_}
+    out["pivot"] = int(d_info.item())
+    return X, out, status
