@@ -1,0 +1,373 @@
+"""Headline benchmark: mixed-precision refined SPD solve vs plain FP64, n = 32768, 64 RHS.
+
+One step = one solve of A X = B through the library's C-ABI (rc_spd_solve_mixed): FP32
+working copy with TF32 (default) or BF16 tensor-core trailing updates and FP64 diagonal
+blocks, then FP64 conjugate-gradient refinement to a normwise backward error <= 1e-15.
+Inputs: A = Q diag(lambda) Q^T, Q from the QR of a seeded N(0,1) matrix, lambda
+log-spaced from 1 to 1/kappa; B ~ N(0,1), 64 columns (synthetic, seeded; generated on the
+GPU by torch -- input generation only, outside every timed region).
+
+metric unit: TFLOP/s counted as n^3/3 + 2 n^2 nrhs per solve (refinement flops are not
+credited), for the mixed solve and the plain FP64 solve alike.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--n 32768] [--nrhs 64] [--kappa 1e2] [--precision tf32|bf16]
+
+--impl reference times the reference's own CPU path (Remora's cholesky_decomposition +
+solve, compiled from its headers into oracle/_ref) on the host cores, on a bounded
+sample of the workload (n = 4096 by default), in the same metric. For N > 1 GPUs each rank
+runs an independent replica (the path does not shard: replicas only); the time is the
+max over ranks and value counts all ranks' solves.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SPD solve TFLOP/s n=32768 mixed+refine vs plain FP64, equal backward error"
+
+
+def flops(n: int, nrhs: int) -> float:
+    return n ** 3 / 3.0 + 2.0 * n * n * nrhs
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        d["source"] = "measured"
+        return d
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = open(f"/tmp/rc_clocks_{os.getpid()}.csv", "w+")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if self.out is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.count(",") >= 8]
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_spd(n: int, kappa: float, seed: int, device):
+    """A = Q diag(lambda) Q^T (column-major FP64), Q from the QR of a seeded Gaussian."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    G = torch.randn((n, n), generator=g, device=device, dtype=torch.float64)
+    Q, _ = torch.linalg.qr(G)
+    del G
+    lam = torch.logspace(0.0, -math.log10(kappa), n, device=device, dtype=torch.float64)
+    A = (Q * lam) @ Q.T
+    del Q
+    A = (A + A.T) * 0.5  # exactly symmetric
+    torch.cuda.synchronize()
+    return A  # symmetric, so its row-major storage is also its column-major storage
+
+
+def backward_error(A, X, B) -> float:
+    import torch
+    R = B - A @ X
+    normA = A.abs().sum(dim=0).max()
+    eta = R.abs().amax(dim=0) / (normA * X.abs().amax(dim=0) + B.abs().amax(dim=0))
+    return float(eta.max().item())
+
+
+def cpu_reference(n: int, nrhs: int, steps: int, warmup: int, seed: int = 1) -> dict:
+    """The reference's CPU path (oracle/_ref: Remora's cholesky_decomposition + solve),
+    single-threaded as the reference is, on an n x n SPD sample of the workload."""
+    import numpy as np
+    import oracle
+    ref = oracle.Reference()
+    g = ref.rng(seed)
+    G = g.normal(n, n)
+    A = np.asfortranarray(G @ G.T / n + 1e-2 * np.eye(n))
+    B = g.normal(n, nrhs, row_major=False)
+    times = []
+    for i in range(warmup + steps):
+        X = np.array(B, order="F")
+        t0 = time.perf_counter()
+        status = ref.cholesky_solve(A, X)
+        dt = time.perf_counter() - t0
+        assert status == 0
+        if i >= warmup:
+            times.append(dt)
+    t = min(times)
+    return {"value": flops(n, nrhs) / t / 1e12, "seconds": t, "times": times}
+
+
+def run_reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n = args.ref_n
+    r = cpu_reference(n, args.nrhs, args.steps, args.warmup)
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"cholesky_decomposition + solve (FP64), n={n} sample of n=32768, nrhs={args.nrhs}",
+                   "n": n, "nrhs": args.nrhs, "flops_per_step": flops(n, args.nrhs)},
+        "impl": "reference",
+        "cpu_baseline": {"value": r["value"], "unit": "TFLOP/s", "cores": 1, "kind": "reference",
+                         "sample": f"one FP64 SPD solve n={n}, nrhs={args.nrhs} (min of {args.steps})",
+                         "host_cores": os.cpu_count()},
+        "e2e": {"value": r["value"], "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+    from remora_b200 import _lib, ops
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    lib = _lib.lib()
+    n, nrhs = args.n, args.nrhs
+    A = make_spd(n, args.kappa, seed=1234 + rank, device=dev)
+    gB = torch.Generator(device=dev).manual_seed(99 + rank)
+    B = torch.randn((nrhs, n), generator=gB, device=dev, dtype=torch.float64).t()  # column-major
+    X = torch.empty((nrhs, n), device=dev, dtype=torch.float64).t()
+    stream = torch.cuda.current_stream()
+
+    def step():
+        _, info, status = ops.spd_solve_mixed(A, B, args.precision, tol=1e-15, max_iter=args.max_iter, X=X)
+        return info, status
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        info, status = step()
+    barrier()
+    launches0 = lib.rc_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    infos = []
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            infos.append(step())
+        e1.record(stream)
+        barrier()
+    launches = lib.rc_launch_count() - launches0
+    t = e0.elapsed_time(e1) / 1e3
+    tmax = torch.tensor([t], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    t = float(tmax.item())
+    mixed_bwd = backward_error(A, X, B)
+    status_ok = all(s == 0 for _, s in infos)
+    last = infos[-1][0]
+
+    # Plain FP64 solve (this library) and the cuSOLVER comparator, same inputs.
+    X64 = B.clone()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    st64 = ops.cholesky_solve(A, X64)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t64 = e0.elapsed_time(e1) / 1e3
+    fp64_bwd = backward_error(A, X64, B)
+    del X64
+    torch.cuda.empty_cache()
+    e0.record(stream)
+    L, _ = torch.linalg.cholesky_ex(A)
+    Xc = torch.cholesky_solve(B, L)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    tcus = e0.elapsed_time(e1) / 1e3
+    cus_bwd = backward_error(A, Xc, B)
+    del L, Xc
+    torch.cuda.empty_cache()
+
+    # End to end through the C-ABI from pinned host buffers: H2D of A and B, the solve,
+    # D2H of X, every step.
+    e2e = None
+    if not args.no_e2e:
+        Ah = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+        Ah.copy_(A)
+        Bh = B.cpu().pin_memory()
+        Xh = torch.empty((nrhs, n), dtype=torch.float64, pin_memory=True).t()
+        Ad = torch.empty_like(A)
+        Bd = torch.empty((nrhs, n), device=dev, dtype=torch.float64).t()
+        del A
+        torch.cuda.empty_cache()
+        torch.cuda.synchronize()
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            Ad.copy_(Ah, non_blocking=True)
+            Bd.copy_(Bh, non_blocking=True)
+            ops.spd_solve_mixed(Ad, Bd, args.precision, tol=1e-15, max_iter=args.max_iter, X=X)
+            Xh.copy_(X, non_blocking=True)
+        e1.record(stream)
+        barrier()
+        te = torch.tensor([e0.elapsed_time(e1) / 1e3], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        te = float(te.item())
+        e2e = {"value": world * args.steps * flops(n, nrhs) / te / 1e12, "unit": "TFLOP/s",
+               "h2d_bytes_per_step": n * n * 8 + n * nrhs * 8, "d2h_bytes_per_step": n * nrhs * 8,
+               "ms_per_step": te / args.steps * 1e3}
+        del Ah, Ad
+        torch.cuda.empty_cache()
+    else:
+        del A
+
+    # Roofline: the dominant kernel, the tcgen05 trailing update (lower SYRK C -= P P^T)
+    # at the largest trailing shape of the factorisation, timed alone with CUDA events.
+    outer = 1024
+    rows = n - outer
+    peaks = load_peaks()
+    prec = 1 if args.precision == "bf16" else 0
+    esz = 2 if prec else 4
+    P = torch.randn((rows, outer), device=dev, dtype=torch.float32)
+    if prec:
+        P = P.bfloat16()
+    C = torch.zeros((rows, rows), device=dev, dtype=torch.float32)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+
+    def syrk():
+        _lib.call("rc_syrk_tc", prec, rows, outer, -1.0, ctypes.c_void_p(P.data_ptr()), outer, 1.0,
+                  ctypes.c_void_p(C.data_ptr()), rows, sptr)
+
+    for _ in range(3):
+        syrk()
+    torch.cuda.synchronize()
+    reps = 10
+    e0.record(stream)
+    for _ in range(reps):
+        syrk()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    tk = e0.elapsed_time(e1) / 1e3 / reps
+    syrk_flops = float(rows) * (rows + 1) * outer
+    achieved = syrk_flops / tk / 1e12
+    peak = peaks["bf16_tflops"] if prec else peaks["bf16_tflops"] / 2.0
+    del P, C
+    torch.cuda.empty_cache()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            r = cpu_reference(args.ref_n, nrhs, steps=1, warmup=0)
+            cpu = {"value": r["value"], "unit": "TFLOP/s", "cores": 1, "kind": "reference",
+                   "sample": f"Remora CPU cholesky_decomposition + solve, n={args.ref_n}, nrhs={nrhs}, one run",
+                   "host_cores": os.cpu_count()}
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "unit": "TFLOP/s", "cores": 1, "kind": "reference", "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": world * args.steps * flops(n, nrhs) / t / 1e12,
+            "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (factor: fp32 storage, " + args.precision + " tensor products)",
+            "data": "synthetic (seeded Q diag(lambda) Q^T, N(0,1) right-hand sides)",
+            "config": {"workload": f"mixed-precision refined SPD solve n={n} nrhs={nrhs} kappa={args.kappa:g}",
+                       "n": n, "nrhs": nrhs, "kappa": args.kappa, "precision": args.precision,
+                       "tol": 1e-15, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (A is n^2 x 8 bytes)"},
+            "mixed": {"converged": status_ok, "backward_error": mixed_bwd, "cg_iterations": last["iterations"],
+                      "factor_ms": last["factor_ms"], "refine_ms": last["refine_ms"], "shift": last["shift"]},
+            "fp64_plain": {"ms": t64 * 1e3, "tflops": flops(n, nrhs) / t64 / 1e12, "backward_error": fp64_bwd,
+                           "status": st64},
+            "fp64_cusolver": {"ms": tcus * 1e3, "tflops": flops(n, nrhs) / tcus / 1e12, "backward_error": cus_bwd},
+            "speedup_vs_fp64_plain": t64 / (t / args.steps),
+            "speedup_vs_cusolver": tcus / (t / args.steps),
+            "roofline": {"kernel": f"tc_gemm_kernel (lower SYRK {rows}x{rows}x{outer}, {args.precision})",
+                         "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": ("bf16_tflops of " if prec else "bf16_tflops/2 (TF32 rate) of ")
+                         + peaks.get("source", "?") + " peaks",
+                         "algorithmic": "n(n+1)k flops per launch"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=32768)
+    ap.add_argument("--nrhs", type=int, default=64)
+    ap.add_argument("--kappa", type=float, default=1e2)
+    ap.add_argument("--precision", choices=["tf32", "bf16"], default="tf32")
+    ap.add_argument("--max-iter", type=int, default=200)
+    ap.add_argument("--ref-n", type=int, default=4096, help="CPU reference sample size")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

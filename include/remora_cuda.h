@@ -37,6 +37,8 @@ enum {
 int rc_version(void);
 /* Static description of a status code. */
 const char* rc_error_string(int status);
+/* Number of kernels the library has launched so far in this process (all devices). */
+unsigned long long rc_launch_count(void);
 /* Free every cached workspace of the current device (synchronises the device). */
 int rc_release_workspaces(void);
 /* Failure detection. Every device-side wait (mbarrier phases of the tensor-core
@@ -135,7 +137,7 @@ int rc_spd_solve_f64(size_t n, size_t nrhs, const double* A, size_t lda, double*
  * Mixed-precision refined SPD solve (extension; no reference counterpart -- the reference
  * solves SPD systems only in the working precision, decompositions.hpp:81-105).
  * X = A^-1 B for a symmetric positive definite A given in FULL (both triangles), FP64:
- *  - factor S A S + theta I (S = diag(A)^-1/2, theta = shift_factor * u_f) in FP32 storage
+ *  - factor S A S + theta I (S = diag(A)^-1/2, theta a multiple of u_f) in FP32 storage
  *    with FP64 diagonal blocks and TF32 or BF16 tensor-core trailing updates (FP32
  *    accumulation);
  *  - refine in FP64 (FP64 residuals and products) by preconditioned conjugate gradients
@@ -149,7 +151,8 @@ typedef struct {
     double tol;          /* backward-error target (<= 0: 1e-15) */
     int max_iter;        /* CG iterations allowed in total (< 0: 100) */
     int outer;           /* outer panel width, a multiple of 128 (<= 0: 1024) */
-    double shift_factor; /* theta = shift_factor * u_f (< 0: 1) */
+    double shift_factor; /* theta = shift_factor * u_f; < 0: adaptive (0, then 1, 8, 64 u_f
+                            after a breakdown of the low-precision factorisation) */
 } rc_mixed_options;
 typedef struct {
     int iterations;        /* preconditioned CG iterations */
@@ -164,6 +167,14 @@ int rc_spd_solve_mixed(int precision, size_t n, size_t nrhs, const double* A, si
                        const double* B, size_t ldb, double* X, size_t ldx,
                        const rc_mixed_options* options, int* d_info, rc_refine_info* info,
                        void* stream);
+/* The trailing update of the mixed-precision factorisation as a standalone call: the
+ * lower triangle of the row-major n x n FP32 matrix C (element (i, j), j <= i, at
+ * C[i * ldc + j]) <- alpha * P P^T + beta * C on the tcgen05 tensor cores, with P a
+ * row-major n x k matrix of FP32 (RC_PREC_TF32) or BF16 (RC_PREC_BF16) elements, rows
+ * 16-byte aligned. The strictly upper triangle is not touched. (A lower-triangle SYRK,
+ * kernels::syrk<false> of include/remora/kernels/syrk.hpp:55-67, in reduced precision.) */
+int rc_syrk_tc(int precision, size_t n, size_t k, float alpha, const void* P, size_t ldp,
+               float beta, float* C, size_t ldc, void* stream);
 /* Device workspace the solve caches for these sizes, in bytes. */
 int rc_spd_solve_mixed_workspace(int precision, size_t n, size_t nrhs,
                                  const rc_mixed_options* options, size_t* bytes);

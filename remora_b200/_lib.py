@@ -37,6 +37,7 @@ SIGNATURES: dict[str, list] = {
     "rc_version": [],
     "rc_error_string": [_I],
     "rc_release_workspaces": [],
+    "rc_launch_count": [],
     "rc_rng_bits_u32": [_U4, _Z, _Z, _P, _Z, _I, _P],
     "rc_rng_uniform_f32": [_U4, _Z, _Z, _P, _Z, _I, c_float, c_float, _P],
     "rc_rng_normal_f32": [_U4, _Z, _Z, _P, _Z, _I, c_float, c_float, _P],
@@ -58,12 +59,13 @@ SIGNATURES: dict[str, list] = {
     "rc_spd_solve_f64": [_Z, _Z, _P, _Z, _P, _Z, _P, _P],
     "rc_spd_solve_mixed": [_I, _Z, _Z, _P, _Z, _P, _Z, _P, _Z, _P, _P, _P, _P],
     "rc_spd_solve_mixed_workspace": [_I, _Z, _Z, _P, _P],
+    "rc_syrk_tc": [_I, _Z, _Z, c_float, _P, _Z, c_float, _P, _Z, _P],
     "rc_copy2d_f64": [_I, _Z, _Z, c_double, _P, _Z, _P, _Z, _P],
     "rc_copy2d_f32": [_I, _Z, _Z, c_float, _P, _Z, _P, _Z, _P],
     "rc_fill_f64": [_Z, _Z, c_double, _P, _Z, _P],
     "rc_fill_f32": [_Z, _Z, c_float, _P, _Z, _P],
 }
-_RESTYPES = {"rc_error_string": ctypes.c_char_p}
+_RESTYPES = {"rc_error_string": ctypes.c_char_p, "rc_launch_count": ctypes.c_ulonglong}
 
 _lib = None
 

@@ -1,5 +1,6 @@
 // Library-wide host helpers: status strings, SM count and the cached workspaces.
 #include "common.cuh"
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -75,6 +76,11 @@ int* error_word() {
     return w;
 }
 
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 uint64_t wait_limit_ns() { return g_wait_limit_ns; }
 void set_wait_limit_ns(uint64_t ns) { g_wait_limit_ns = ns; }
 
@@ -83,6 +89,8 @@ void set_wait_limit_ns(uint64_t ns) { g_wait_limit_ns = ns; }
 extern "C" {
 
 int rc_version(void) { return 100; }
+
+unsigned long long rc_launch_count(void) { return rc::g_launches.load(std::memory_order_relaxed); }
 
 int rc_set_wait_limit_ns(uint64_t ns) {
     if (ns == 0) return RC_ERR_INVALID_ARGUMENT;

@@ -23,7 +23,11 @@ struct View {
 template <class T>
 inline View<T> colmajor(T* p, int64_t ld) { return {p, 1, ld}; }
 
+// Count of kernels this library has launched (every launch is followed by check_launch).
+void count_launch();
+
 inline int check_launch() {
+    count_launch();
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? RC_SUCCESS : RC_ERR_CUDA;
 }

@@ -281,12 +281,14 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     o.max_iter = 100;
     o.outer = 1024;
     o.shift_factor = -1.0;
-    if (opt) o = *opt;
+    if (opt) o = *opt;  // shift_factor < 0 selects the adaptive shift
     if (o.outer <= 0 || o.outer % kNB) o.outer = 1024;
     if (o.tol <= 0) o.tol = 1e-15;
     if (o.max_iter < 0) o.max_iter = 100;
     const double uf = prec == RC_PREC_BF16 ? std::ldexp(1.0, -8) : std::ldexp(1.0, -11);
-    const double theta = (o.shift_factor >= 0.0 ? o.shift_factor : 1.0) * uf;
+    // shift_factor < 0: adaptive -- no shift first, then 1, 8, 64 u_f after a breakdown.
+    const bool adaptive = o.shift_factor < 0.0;
+    double theta = adaptive ? 0.0 : o.shift_factor * uf;
 
     size_t bytes = 0;
     mixed_workspace_bytes(n, nrhs, prec, o.outer, &bytes);
@@ -314,19 +316,24 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     cudaEvent_t e0, e1, e2;
     cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
     cudaEventRecord(e0, s);
-    if (cudaMemsetAsync(d_info, 0, sizeof(int), s) != cudaSuccess) return RC_ERR_CUDA;
     const View<const double> Av = M.Av();
     diag_scale_kernel<<<ceil_div(n, 256) < 1024u ? ceil_div(n, 256) : 1024u, 256, 0, s>>>(n, Av, M.sc);
     RC_TRY(check_launch());
-    scale_to_f32_kernel<<<dim3(ceil_div(n, 32), ceil_div(n, 32)), 256, 0, s>>>(n, Av, M.sc, theta, M.W, M.ldw);
-    RC_TRY(check_launch());
-    RC_TRY(M.factor(o.outer, d_info));
-    cudaEventRecord(e1, s);
     int h_info = 0;
-    if (cudaMemcpyAsync(&h_info, d_info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess)
-        return RC_ERR_CUDA;
+    for (int attempt = 0;; ++attempt) {
+        if (cudaMemsetAsync(d_info, 0, sizeof(int), s) != cudaSuccess) return RC_ERR_CUDA;
+        scale_to_f32_kernel<<<dim3(ceil_div(n, 32), ceil_div(n, 32)), 256, 0, s>>>(n, Av, M.sc, theta, M.W, M.ldw);
+        RC_TRY(check_launch());
+        RC_TRY(M.factor(o.outer, d_info));
+        if (cudaMemcpyAsync(&h_info, d_info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return RC_ERR_CUDA;
+        if (h_info == 0 || !adaptive || attempt == 3) break;
+        theta = (attempt == 0 ? 1.0 : attempt == 1 ? 8.0 : 64.0) * uf;
+    }
+    cudaEventRecord(e1, s);
     rc_refine_info info = {};
+    info.shift = theta;
     if (h_info != 0) {
         if (out) *out = info;
         return RC_SUCCESS;  // d_info reports the failing pivot of the low-precision factor

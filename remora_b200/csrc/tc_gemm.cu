@@ -356,6 +356,16 @@ int rc_gemm_bf16(int transA, int transB, size_t m, size_t n, size_t k, float alp
                               rc::colmajor(C, (int64_t)ldc), rc::kFull, 0, s);
 }
 
+int rc_syrk_tc(int precision, size_t n, size_t k, float alpha, const void* P, size_t ldp, float beta, float* C,
+               size_t ldc, void* stream) {
+    if (precision != RC_PREC_TF32 && precision != RC_PREC_BF16) return RC_ERR_INVALID_ARGUMENT;
+    if (n == 0) return RC_SUCCESS;
+    if (!C || ldc < n || (k > 0 && (!P || ldp < k))) return RC_ERR_INVALID_ARGUMENT;
+    return rc::gemm_tc_kmajor(precision == RC_PREC_BF16, (int64_t)n, (int64_t)n, (int64_t)k, alpha, P, (int64_t)ldp, P,
+                              (int64_t)ldp, beta, rc::View<float>{C, (int64_t)ldc, 1}, rc::kLower, 0,
+                              static_cast<cudaStream_t>(stream));
+}
+
 int rc_selftest_wait_timeout(uint64_t limit_ns, void* stream) {
     int* err = rc::error_word();
     if (!err) return RC_ERR_ALLOC;
