@@ -30,7 +30,8 @@ enum {
     RC_ERR_ALLOC = 3,            /* a workspace allocation failed */
     RC_ERR_NOT_SUPPORTED = 4,    /* a combination the library does not implement */
     RC_ERR_TIMEOUT = 5,          /* a bounded device-side wait gave up */
-    RC_ERR_NOT_CONVERGED = 6     /* iterative refinement did not reach its tolerance */
+    RC_ERR_NOT_CONVERGED = 6,    /* iterative refinement did not reach its tolerance */
+    RC_ERR_SIZE_LIMIT = 7        /* the problem exceeds an entry point's fixed scratch */
 };
 
 /* Library version (major * 10000 + minor * 100 + patch). */
@@ -132,6 +133,19 @@ int rc_potrf_f32(int upper, size_t n, float* A, size_t lda, int* d_info, void* s
  * in rc_potrf_*; on failure B is left unchanged. */
 int rc_spd_solve_f64(size_t n, size_t nrhs, const double* A, size_t lda, double* B, size_t ldb,
                      int* d_info, void* stream);
+
+/* The same solve without any device allocation, for callers that cannot let a library
+ * allocate while they run: services whose device memory is reserved up front by their
+ * own pool allocator, and latency-bound loops where cudaMalloc/cudaFree (which can
+ * synchronise the device) are not allowed. No counterpart in the reference. Scratch is
+ * one 9.19 MiB __device__ array inside the library, held by every GPU that loads it until
+ * the process exits: n <= 1024 and nrhs <= 64, else RC_ERR_SIZE_LIMIT. The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture. All calls share the array: calls whose work overlaps
+ * on the GPU (other streams, other host threads) race on it. d_info, A and B as in
+ * rc_spd_solve_f64. */
+int rc_spd_solve_f64_noalloc(size_t n, size_t nrhs, const double* A, size_t lda, double* B,
+                             size_t ldb, int* d_info, void* stream);
 
 /* ---------------------------------------------------------------------------------
  * Mixed-precision refined SPD solve (extension; no reference counterpart -- the reference

@@ -25,7 +25,7 @@ class RefineInfo(ctypes.Structure):
     _fields_ = [("iterations", c_int), ("residuals", c_int), ("converged", c_int), ("backward_error", c_double),
                 ("factor_ms", c_double), ("refine_ms", c_double), ("shift", c_double)]
 STATUS_NAMES = {0: "RC_SUCCESS", 1: "RC_ERR_INVALID_ARGUMENT", 2: "RC_ERR_CUDA", 3: "RC_ERR_ALLOC",
-                4: "RC_ERR_NOT_SUPPORTED", 5: "RC_ERR_TIMEOUT", 6: "RC_ERR_NOT_CONVERGED"}
+                4: "RC_ERR_NOT_SUPPORTED", 5: "RC_ERR_TIMEOUT", 6: "RC_ERR_NOT_CONVERGED", 7: "RC_ERR_SIZE_LIMIT"}
 
 _U4 = POINTER(c_uint32)
 _I = c_int
@@ -57,6 +57,7 @@ SIGNATURES: dict[str, list] = {
     "rc_potrf_f64": [_I, _Z, _P, _Z, _P, _P],
     "rc_potrf_f32": [_I, _Z, _P, _Z, _P, _P],
     "rc_spd_solve_f64": [_Z, _Z, _P, _Z, _P, _Z, _P, _P],
+    "rc_spd_solve_f64_noalloc": [_Z, _Z, _P, _Z, _P, _Z, _P, _P],
     "rc_spd_solve_mixed": [_I, _Z, _Z, _P, _Z, _P, _Z, _P, _Z, _P, _P, _P, _P],
     "rc_spd_solve_mixed_workspace": [_I, _Z, _Z, _P, _P],
     "rc_syrk_tc": [_I, _Z, _Z, c_float, _P, _Z, c_float, _P, _Z, _P],

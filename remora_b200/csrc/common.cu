@@ -107,6 +107,7 @@ const char* rc_error_string(int status) {
     case RC_ERR_NOT_SUPPORTED: return "combination not supported";
     case RC_ERR_TIMEOUT: return "a bounded device-side wait gave up";
     case RC_ERR_NOT_CONVERGED: return "iterative refinement did not converge";
+    case RC_ERR_SIZE_LIMIT: return "problem larger than the entry point's fixed scratch";
     default: return "unknown status";
     }
 }

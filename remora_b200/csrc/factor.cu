@@ -230,6 +230,15 @@ int trsm_preinv(bool trans, int64_t m, int64_t n, View<const T> L, const T* Winv
     return RC_SUCCESS;
 }
 
+template <class T>
+int trtri_blocks_launch(int64_t m, View<const T> L, bool unit, T* W, int* info, const int* abort, cudaStream_t s) {
+    if (m <= 0) return RC_SUCCESS;
+    RC_TRY(set_smem(trtri_blocks<T>, kBlockSmem));
+    trtri_blocks<T><<<(unsigned)((m + NB - 1) / NB), NB, kBlockSmem, s>>>(m, L, unit, W, info, abort);
+    return check_launch();
+}
+
+template int trtri_blocks_launch<double>(int64_t, View<const double>, bool, double*, int*, const int*, cudaStream_t);
 template int potrf_diag_block<float>(View<float>, int, int64_t, float*, bool, int*, cudaStream_t);
 template int potrf_diag_block<double>(View<double>, int, int64_t, double*, bool, int*, cudaStream_t);
 template int trsm_preinv<float>(bool, int64_t, int64_t, View<const float>, const float*, View<float>, float*,

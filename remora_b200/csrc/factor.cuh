@@ -44,4 +44,9 @@ int potrf_diag_block(View<T> A, int sz, int64_t g0, T* W, bool w_row_major, int*
 template <class T>
 int trsm_preinv(bool trans, int64_t m, int64_t n, View<const T> L, const T* Winv, View<T> B, T* tmp, cudaStream_t s);
 
+// Invert every kNB x kNB diagonal block of the lower-triangular m x m view L into W
+// (column-major kNB x kNB blocks, block b at W + b * kNB * kNB); skipped when *abort != 0.
+template <class T>
+int trtri_blocks_launch(int64_t m, View<const T> L, bool unit, T* W, int* info, const int* abort, cudaStream_t s);
+
 }  // namespace rc
