@@ -86,43 +86,122 @@ __global__ void __launch_bounds__(NB) trtri_blocks(int64_t m, View<const T> L, b
     store_block<T>(S, W + (size_t)blockIdx.x * NB * NB);
 }
 
-// Factor the sz x sz lower diagonal block (A already offset to it) in FP64 shared
-// memory, write L back, and store inv(L) into W. g0 = global index of the block.
+// Factor the sz x sz lower diagonal block (A already offset to it) in FP64 and store
+// inv(L) into W (column-major, or row-major when w_row_major); g0 = global index of the
+// block for the pivot status. Register-blocked: thread (ty, tx) of the 16 x 16 CTA owns
+// the 8 x 8 elements (ty + 16 r, tx + 16 q) in registers; each column step broadcasts one
+// column through shared memory (two barriers per column), and the inverse is formed the
+// same way by right-looking forward substitution on the identity (one barrier per row,
+// double-buffered row broadcast).
 template <class T>
-__global__ void __launch_bounds__(256) potrf_diag(View<T> A, int sz, int64_t g0, T* W, int* info,
-                                                  bool w_row_major) {
-    extern __shared__ double S[];
+__global__ void __launch_bounds__(256, 1) potrf_diag(View<T> A, int sz, int64_t g0, T* W, int* info,
+                                                     bool w_row_major) {
+    extern __shared__ double S[];  // NB x SLD: L after the factorisation
+    __shared__ double col[NB];
+    __shared__ double row2[2][NB];
+    __shared__ double piv;
     if (aborted(info)) return;
-    const int tid = threadIdx.x;
-    for (int e = tid; e < NB * NB; e += blockDim.x) {
-        const int i = e % NB, j = e / NB;
-        S[i * SLD + j] = (i < sz && j < sz && j <= i) ? (double)A(i, j) : (i == j ? 1.0 : 0.0);
-    }
-    __syncthreads();
-    for (int j = 0; j < sz; ++j) {
-        const double d = S[j * SLD + j];
-        if (!(d > 0.0)) {  // also catches NaN
-            if (tid == 0) record_first(info, (int)(g0 + j + 1));
-            return;
+    const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+    double a[8][8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int i = ty + 16 * r, c = tx + 16 * q;
+            a[r][q] = (i < sz && c < sz && c <= i) ? (double)A(i, c) : (i == c ? 1.0 : 0.0);
         }
-        const double sq = sqrt(d);
-        __syncthreads();
-        for (int i = j + tid; i < sz; i += blockDim.x) S[i * SLD + j] = (i == j) ? sq : S[i * SLD + j] / sq;
-        __syncthreads();
-        const int t = sz - j - 1;
-        for (int e = tid; e < t * t; e += blockDim.x) {
-            const int i = j + 1 + e / t, c = j + 1 + e % t;
-            if (c <= i) S[i * SLD + c] = fma(-S[i * SLD + j], S[c * SLD + j], S[i * SLD + c]);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        for (int jj = 0; jj < 16; ++jj) {
+            const int j = 16 * q + jj;
+            if (j >= sz) break;
+            if (tx == jj && ty == jj) {
+                const double d = a[q][q];
+                piv = d > 0.0 ? sqrt(d) : -1.0;  // also catches NaN
+            }
+            __syncthreads();
+            const double sq = piv;
+            if (!(sq > 0.0)) {
+                if (tid == 0) record_first(info, (int)(g0 + j + 1));
+                return;
+            }
+            if (tx == jj) {
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    const int i = ty + 16 * r;
+                    double v = 0.0;
+                    if (i == j) v = sq;
+                    else if (i > j) v = a[r][q] / sq;
+                    if (i >= j) a[r][q] = v;
+                    col[i] = v;
+                }
+            }
+            __syncthreads();
+            double lr[8], lc[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) lr[r] = col[ty + 16 * r];
+#pragma unroll
+            for (int q2 = 0; q2 < 8; ++q2) lc[q2] = col[tx + 16 * q2];
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+#pragma unroll
+                for (int q2 = 0; q2 < 8; ++q2) {
+                    const int i = ty + 16 * r, c = tx + 16 * q2;
+                    if (c > j && i >= c) a[r][q2] = fma(-lr[r], lc[q2], a[r][q2]);
+                }
         }
-        __syncthreads();
     }
-    for (int e = tid; e < NB * NB; e += blockDim.x) {
-        const int i = e % NB, j = e / NB;
-        if (i < sz && j <= i) A(i, j) = (T)S[i * SLD + j];
-    }
+    // L back to global memory (lower part) and to shared memory for the inversion.
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int i = ty + 16 * r, c = tx + 16 * q;
+            const double v = c <= i ? a[r][q] : 0.0;
+            S[i * SLD + c] = v;
+            if (i < sz && c <= i) A(i, c) = (T)v;
+        }
+    // Padding rows/columns beyond sz hold the identity, so the inverse is well defined.
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) a[r][q] = (ty + 16 * r == tx + 16 * q) ? 1.0 : 0.0;
     __syncthreads();
-    invert_lower_inplace(S, false);
-    store_block<T>(S, W, w_row_major);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        for (int kk = 0; kk < 16; ++kk) {
+            const int k = 16 * q + kk;
+            double* rb = row2[k & 1];
+            if (ty == kk) {
+                const double inv = 1.0 / S[k * SLD + k];
+#pragma unroll
+                for (int q2 = 0; q2 < 8; ++q2) {
+                    a[q][q2] *= inv;
+                    rb[tx + 16 * q2] = a[q][q2];
+                }
+            }
+            __syncthreads();
+            double xr[8];
+#pragma unroll
+            for (int q2 = 0; q2 < 8; ++q2) xr[q2] = rb[tx + 16 * q2];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const int i = ty + 16 * r;
+                if (i > k) {
+                    const double l = S[i * SLD + k];
+#pragma unroll
+                    for (int q2 = 0; q2 < 8; ++q2) a[r][q2] = fma(-l, xr[q2], a[r][q2]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int i = ty + 16 * r, c = tx + 16 * q;
+            W[w_row_major ? i * NB + c : c * NB + i] = c <= i ? (T)a[r][q] : T(0);
+        }
 }
 
 template <class K>
@@ -181,23 +260,37 @@ int potrf_lower(int64_t n, View<T> A, int* info, cudaStream_t s) {
         if (!tmp) return RC_ERR_ALLOC;
     }
     RC_TRY(set_smem(potrf_diag<T>, kBlockSmem));
-    const View<const T> Wt = {W, NB, 1};  // inv(L_kk)^T
-    for (int64_t k0 = 0; k0 < n; k0 += NB) {
-        const int sz = (int)((n - k0) < NB ? n - k0 : NB);
-        potrf_diag<T><<<1, 256, kBlockSmem, s>>>(A.sub(k0, k0), sz, k0, W, info, false);
-        RC_TRY(check_launch());
-        const int64_t rows = n - k0 - sz;
-        if (rows <= 0) break;
-        View<T> P = A.sub(k0 + sz, k0);
-        const View<const T> Pc = {P.p, P.rs, P.cs};
-        if (in_place) {
-            RC_TRY(gemm<T>(rows, sz, sz, T(1), Pc, Wt, T(0), P, kFull, 0, s, info));
-        } else {
-            const View<T> Tv = colmajor(tmp, rows);
-            RC_TRY(gemm<T>(rows, sz, sz, T(1), Pc, Wt, T(0), Tv, kFull, 0, s, info));
-            RC_TRY(copy2d<T, T>(rows, sz, T(1), View<const T>{Tv.p, Tv.rs, Tv.cs}, P, s, info));
+    const View<const T> Wt = {W, NB, 1};  // inv(L_jj)^T
+    // Outer panels of kOuter columns: inner 128-column blocks update only the rest of
+    // their panel, and the trailing matrix gets one update of depth kOuter per panel, so
+    // the dominant GEMM streams its C tiles kOuter / 128 times less often.
+    constexpr int64_t kOuter = 512;
+    auto C_ = [](const View<T>& v) { return View<const T>{v.p, v.rs, v.cs}; };
+    for (int64_t k0 = 0; k0 < n; k0 += kOuter) {
+        const int64_t w = (n - k0) < kOuter ? n - k0 : kOuter;
+        for (int64_t j0 = k0; j0 < k0 + w; j0 += NB) {
+            const int jb = (int)((k0 + w - j0) < NB ? k0 + w - j0 : NB);
+            potrf_diag<T><<<1, 256, kBlockSmem, s>>>(A.sub(j0, j0), jb, j0, W, info, false);
+            RC_TRY(check_launch());
+            const int64_t rows = n - j0 - jb;
+            if (rows <= 0) continue;
+            View<T> P = A.sub(j0 + jb, j0);
+            if (in_place) {
+                RC_TRY(gemm<T>(rows, jb, jb, T(1), C_(P), Wt, T(0), P, kFull, 0, s, info));
+            } else {
+                const View<T> Tv = colmajor(tmp, rows);
+                RC_TRY(gemm<T>(rows, jb, jb, T(1), C_(P), Wt, T(0), Tv, kFull, 0, s, info));
+                RC_TRY(copy2d<T, T>(rows, jb, T(1), C_(Tv), P, s, info));
+            }
+            const int64_t cw = k0 + w - (j0 + jb);
+            if (cw > 0)
+                RC_TRY(gemm<T>(rows, cw, jb, T(-1), C_(P), C_(P).t(), T(1), A.sub(j0 + jb, j0 + jb), kLower, 0, s,
+                               info));
         }
-        RC_TRY(gemm<T>(rows, rows, sz, T(-1), Pc, Pc.t(), T(1), A.sub(k0 + sz, k0 + sz), kLower, 0, s, info));
+        const int64_t rows = n - k0 - w;
+        if (rows <= 0) continue;
+        const View<T> Pk = A.sub(k0 + w, k0);
+        RC_TRY(gemm<T>(rows, rows, w, T(-1), C_(Pk), C_(Pk).t(), T(1), A.sub(k0 + w, k0 + w), kLower, 0, s, info));
     }
     return RC_SUCCESS;
 }

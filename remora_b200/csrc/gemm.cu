@@ -93,10 +93,22 @@ __global__ void __launch_bounds__(256) gemm_simt(int64_t m, int64_t n, int64_t k
 }
 
 // ------------------------------------------------------------------------------------
-// FP64 DMMA kernel.
-constexpr int DM = 128, DN = 128, DK = 16, DSTAGES = 3, DPAD = 4;
-constexpr int DLDA = DM + DPAD, DLDB = DN + DPAD;
-constexpr size_t kDmmaSmem = (size_t)DSTAGES * DK * (DLDA + DLDB) * sizeof(double);
+// FP64 DMMA kernel: 128 x BN tiles (BN = 128 or 64 for skinny right-hand sides), k-step 16,
+// 8 warps. gridDim.z > 1 splits K: slice z covers [z * kchunk, (z + 1) * kchunk) and
+// writes its partial product (alpha = 1, beta = 0) to Cz + z * zstride; a second kernel
+// then reduces the slices into C.
+constexpr int DM = 128, DK = 16, DSTAGES = 3, DPAD = 4;
+constexpr int DLDA = DM + DPAD;
+
+template <int BN>
+struct DmmaCfg {
+    static constexpr int LDB = BN + DPAD;
+    static constexpr int WARPS_N = BN == 128 ? 4 : 2;  // warps along N
+    static constexpr int WARPS_M = 8 / WARPS_N;
+    static constexpr int WM = DM / WARPS_M, WN = BN / WARPS_N;  // warp tile
+    static constexpr int MI = WM / 16, NI = WN / 8;
+    static constexpr size_t SMEM = (size_t)DSTAGES * DK * (DLDA + LDB) * sizeof(double);
+};
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -116,10 +128,11 @@ __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1
 
 // A_KMAJOR: A(i, k) is contiguous along k (A.cs == 1), else along i (A.rs == 1).
 // B_KMAJOR: B(k, j) is contiguous along k (B.rs == 1), else along j (B.cs == 1).
-template <bool A_KMAJOR, bool B_KMAJOR>
+template <bool A_KMAJOR, bool B_KMAJOR, int BN>
 __device__ __forceinline__ void dmma_load_tile(double* sA, double* sB, const View<const double>& A,
                                                const View<const double>& B, int64_t m, int64_t n, int64_t k,
                                                int64_t m0, int64_t n0, int64_t k0, int tid) {
+    constexpr int LDB = DmmaCfg<BN>::LDB;
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
         int mm, kk;
@@ -129,33 +142,42 @@ __device__ __forceinline__ void dmma_load_tile(double* sA, double* sB, const Vie
         cp_async8(sA + kk * DLDA + mm, ok ? &A(gi, gk) : A.p, ok);
     }
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
+    for (int r = 0; r < BN / 16; ++r) {
         int nn, kk;
-        if (B_KMAJOR) { kk = tid % 16; nn = tid / 16 + 16 * r; } else { nn = tid % 128; kk = tid / 128 + 2 * r; }
+        if (B_KMAJOR) { kk = tid % 16; nn = tid / 16 + 16 * r; } else { nn = tid % BN; kk = tid / BN + (256 / BN) * r; }
         const int64_t gj = n0 + nn, gk = k0 + kk;
         const bool ok = gj < n && gk < k;
-        cp_async8(sB + kk * DLDB + nn, ok ? &B(gk, gj) : B.p, ok);
+        cp_async8(sB + kk * LDB + nn, ok ? &B(gk, gj) : B.p, ok);
     }
 }
 
-template <bool A_KMAJOR, bool B_KMAJOR>
+template <bool A_KMAJOR, bool B_KMAJOR, int BN>
 __global__ void __launch_bounds__(256, 1) gemm_dmma_f64(int64_t m, int64_t n, int64_t k, double alpha,
                                                          View<const double> A, View<const double> B, double beta,
                                                          View<double> C, Mask mask, int64_t off,
-                                                         const int* abort) {
+                                                         const int* abort, int64_t kchunk, int64_t zstride) {
+    using Cfg = DmmaCfg<BN>;
+    constexpr int LDB = Cfg::LDB, MI = Cfg::MI, NI = Cfg::NI;
     extern __shared__ __align__(16) double dsmem[];
     double* sA = dsmem;
     double* sB = dsmem + DSTAGES * DK * DLDA;
-    const int64_t m0 = (int64_t)blockIdx.y * DM, n0 = (int64_t)blockIdx.x * DN;
-    if (aborted(abort) || tile_outside(mask, off, m0, n0, DM, DN)) return;
+    const int64_t m0 = (int64_t)blockIdx.y * DM, n0 = (int64_t)blockIdx.x * BN;
+    if (aborted(abort) || tile_outside(mask, off, m0, n0, DM, BN)) return;
+    if (gridDim.z > 1) {  // K slice of a split-K product
+        const int64_t kz = (int64_t)blockIdx.z * kchunk;
+        A = A.sub(0, kz);
+        B = B.sub(kz, 0);
+        k = (k - kz) < kchunk ? k - kz : kchunk;
+        C.p += (int64_t)blockIdx.z * zstride;
+    }
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
-    const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;
-    double acc[4][4][4];
+    const int wm = (warp / Cfg::WARPS_N) * Cfg::WM, wn = (warp % Cfg::WARPS_N) * Cfg::WN;
+    double acc[MI][NI][4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < MI; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b)
+        for (int b = 0; b < NI; ++b)
 #pragma unroll
             for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
 
@@ -163,8 +185,8 @@ __global__ void __launch_bounds__(256, 1) gemm_dmma_f64(int64_t m, int64_t n, in
 #pragma unroll
     for (int s = 0; s < DSTAGES - 1; ++s) {
         if (s < KT)
-            dmma_load_tile<A_KMAJOR, B_KMAJOR>(sA + s * DK * DLDA, sB + s * DK * DLDB, A, B, m, n, k, m0, n0,
-                                               (int64_t)s * DK, tid);
+            dmma_load_tile<A_KMAJOR, B_KMAJOR, BN>(sA + s * DK * DLDA, sB + s * DK * LDB, A, B, m, n, k, m0, n0,
+                                                   (int64_t)s * DK, tid);
         cp_async_commit();
     }
     for (int kt = 0; kt < KT; ++kt) {
@@ -173,38 +195,38 @@ __global__ void __launch_bounds__(256, 1) gemm_dmma_f64(int64_t m, int64_t n, in
         const int pf = kt + DSTAGES - 1;
         if (pf < KT) {
             const int st = pf % DSTAGES;
-            dmma_load_tile<A_KMAJOR, B_KMAJOR>(sA + st * DK * DLDA, sB + st * DK * DLDB, A, B, m, n, k, m0, n0,
-                                               (int64_t)pf * DK, tid);
+            dmma_load_tile<A_KMAJOR, B_KMAJOR, BN>(sA + st * DK * DLDA, sB + st * DK * LDB, A, B, m, n, k, m0, n0,
+                                                   (int64_t)pf * DK, tid);
         }
         cp_async_commit();
         const double* a_s = sA + (kt % DSTAGES) * DK * DLDA;
-        const double* b_s = sB + (kt % DSTAGES) * DK * DLDB;
+        const double* b_s = sB + (kt % DSTAGES) * DK * LDB;
 #pragma unroll
         for (int ks = 0; ks < DK; ks += 4) {
-            double af[4][2], bf[4];
+            double af[MI][2], bf[NI];
 #pragma unroll
-            for (int mi = 0; mi < 4; ++mi) {
+            for (int mi = 0; mi < MI; ++mi) {
                 af[mi][0] = a_s[(ks + t) * DLDA + wm + mi * 16 + g];
                 af[mi][1] = a_s[(ks + t) * DLDA + wm + mi * 16 + g + 8];
             }
 #pragma unroll
-            for (int ni = 0; ni < 4; ++ni) bf[ni] = b_s[(ks + t) * DLDB + wn + ni * 8 + g];
+            for (int ni = 0; ni < NI; ++ni) bf[ni] = b_s[(ks + t) * LDB + wn + ni * 8 + g];
 #pragma unroll
-            for (int mi = 0; mi < 4; ++mi)
+            for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
-                for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+                for (int ni = 0; ni < NI; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
         }
     }
     cp_async_wait<0>();
     // Epilogue: element (g, 2t + c) and (g + 8, 2t + c) of each 16x8 accumulator tile.
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi)
+    for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int64_t i = m0 + wm + mi * 16 + g + 8 * h;
             if (i >= m) continue;
 #pragma unroll
-            for (int ni = 0; ni < 4; ++ni)
+            for (int ni = 0; ni < NI; ++ni)
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
                     const int64_t j = n0 + wn + ni * 8 + 2 * t + c;
@@ -216,19 +238,59 @@ __global__ void __launch_bounds__(256, 1) gemm_dmma_f64(int64_t m, int64_t n, in
         }
 }
 
-template <bool AK, bool BK>
+// C = alpha * sum_z P_z + beta * C over the split-K slices (column-major m x n, ld m each).
+__global__ void splitk_reduce(int64_t m, int64_t n, int nz, const double* P, int64_t zstride, double alpha,
+                              double beta, View<double> C) {
+    for (int64_t j = blockIdx.y; j < n; j += gridDim.y)
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+            double acc = 0.0;
+            for (int z = 0; z < nz; ++z) acc += P[z * zstride + i + j * m];
+            double v = alpha * acc;
+            if (beta != 0.0) v = fma(beta, C(i, j), v);
+            C(i, j) = v;
+        }
+}
+
+template <bool AK, bool BK, int BN>
 int launch_dmma(int64_t m, int64_t n, int64_t k, double alpha, View<const double> A, View<const double> B,
                 double beta, View<double> C, Mask mask, int64_t off, cudaStream_t s, const int* abort) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        if (cudaFuncSetAttribute(gemm_dmma_f64<AK, BK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kDmmaSmem) != cudaSuccess)
-            return RC_ERR_CUDA;
-        attr_set = true;
+    const size_t smem = DmmaCfg<BN>::SMEM;
+    if (cudaFuncSetAttribute(gemm_dmma_f64<AK, BK, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return RC_ERR_CUDA;
+    dim3 grid(ceil_div(n, BN), ceil_div(m, DM));
+    // Too few output tiles to fill the GPU and a long K: split K into slices.
+    const int64_t tiles = (int64_t)grid.x * grid.y, sms = sm_count();
+    int nz = 1;
+    if (mask == kFull && k >= 2048 && tiles < sms) {
+        nz = (int)((2 * sms + tiles - 1) / tiles);
+        nz = nz > 16 ? 16 : nz;
+        const int64_t maxz = k / 512;
+        if (nz > maxz) nz = (int)maxz;
     }
-    dim3 grid(ceil_div(n, DN), ceil_div(m, DM));
-    gemm_dmma_f64<AK, BK><<<grid, 256, kDmmaSmem, s>>>(m, n, k, alpha, A, B, beta, C, mask, off, abort);
+    if (nz > 1) {
+        const int64_t kchunk = ((k + nz - 1) / nz + DK - 1) / DK * DK;
+        nz = (int)((k + kchunk - 1) / kchunk);
+        const int64_t zstride = m * n;
+        double* P = static_cast<double*>(workspace(s, (size_t)nz * zstride * sizeof(double), 7));
+        if (!P) return RC_ERR_ALLOC;
+        grid.z = nz;
+        gemm_dmma_f64<AK, BK, BN><<<grid, 256, smem, s>>>(m, n, k, 1.0, A, B, 0.0, colmajor(P, m), kFull, 0, abort,
+                                                          kchunk, zstride);
+        RC_TRY(check_launch());
+        dim3 rg(ceil_div(m, 256) < 1024u ? ceil_div(m, 256) : 1024u, n < 65535 ? (unsigned)n : 65535u);
+        splitk_reduce<<<rg, 256, 0, s>>>(m, n, nz, P, zstride, alpha, beta, C);
+        return check_launch();
+    }
+    gemm_dmma_f64<AK, BK, BN><<<grid, 256, smem, s>>>(m, n, k, alpha, A, B, beta, C, mask, off, abort, k, 0);
     return check_launch();
+}
+
+template <bool AK, bool BK>
+int launch_dmma_bn(int64_t m, int64_t n, int64_t k, double alpha, View<const double> A, View<const double> B,
+                   double beta, View<double> C, Mask mask, int64_t off, cudaStream_t s, const int* abort) {
+    if (n <= 64) return launch_dmma<AK, BK, 64>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
+    return launch_dmma<AK, BK, 128>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
 }
 
 // Scale (beta != 1) the masked part of C when k == 0 or alpha == 0.
@@ -255,10 +317,10 @@ int gemm(int64_t m, int64_t n, int64_t k, T alpha, View<const T> A, View<const T
     if constexpr (std::is_same<T, double>::value) {
         const bool a_k = A.cs == 1, a_m = A.rs == 1, b_k = B.rs == 1, b_n = B.cs == 1;
         if ((a_k || a_m) && (b_k || b_n)) {
-            if (a_k && b_k) return launch_dmma<true, true>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
-            if (a_k) return launch_dmma<true, false>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
-            if (b_k) return launch_dmma<false, true>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
-            return launch_dmma<false, false>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
+            if (a_k && b_k) return launch_dmma_bn<true, true>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
+            if (a_k) return launch_dmma_bn<true, false>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
+            if (b_k) return launch_dmma_bn<false, true>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
+            return launch_dmma_bn<false, false>(m, n, k, alpha, A, B, beta, C, mask, off, s, abort);
         }
     }
     dim3 grid(ceil_div(n, 64), ceil_div(m, 64));

@@ -233,17 +233,52 @@ struct Mixed {
         return RC_SUCCESS;
     }
 
-    // Zout = M^-1 Rin = S L^-T L^-1 S Rin (FP64 in/out, FP32 triangular solves).
-    int precond(const double* Rin, int64_t ldr, double* Zout, int64_t ldz) {
+    // Zout = M^-1 Rin = S L^-T L^-1 S Rin (FP64 in/out, FP32 triangular solves), on st.
+    int precond_on(const double* Rin, int64_t ldr, double* Zout, int64_t ldz, cudaStream_t st) {
         const dim3 g = vec_grid(n, nrhs);
-        to_f32_scaled_kernel<<<g, 256, 0, s>>>(n, nrhs, sc, Rin, ldr, T32);
+        to_f32_scaled_kernel<<<g, 256, 0, st>>>(n, nrhs, sc, Rin, ldr, T32);
         RC_TRY(check_launch());
         const View<const float> L = {W, ldw, 1};
         const View<float> Tv = colmajor(T32, n);
-        RC_TRY(trsm_preinv<float>(false, n, nrhs, L, Winv, Tv, tmp, s));
-        RC_TRY(trsm_preinv<float>(true, n, nrhs, L, Winv, Tv, tmp, s));
-        from_f32_scaled_kernel<<<g, 256, 0, s>>>(n, nrhs, sc, T32, Zout, ldz);
+        RC_TRY(trsm_preinv<float>(false, n, nrhs, L, Winv, Tv, tmp, st));
+        RC_TRY(trsm_preinv<float>(true, n, nrhs, L, Winv, Tv, tmp, st));
+        from_f32_scaled_kernel<<<g, 256, 0, st>>>(n, nrhs, sc, T32, Zout, ldz);
         return check_launch();
+    }
+    int precond(const double* Rin, int64_t ldr, double* Zout, int64_t ldz) {
+        return precond_on(Rin, ldr, Zout, ldz, s);
+    }
+
+    // The CG preconditioner R -> Z is replayed as one CUDA graph: its ~6 n/128 small
+    // launches per application would otherwise be bound by launch latency.
+    cudaGraphExec_t graph_exec = nullptr;
+    size_t graph_kernels = 0;
+    int precond_RZ() {
+        if (!graph_exec) {
+            cudaStream_t cs;
+            if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return RC_ERR_CUDA;
+            const unsigned long long before = rc_launch_count();
+            cudaGraph_t graph = nullptr;
+            int st = RC_SUCCESS;
+            if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed) != cudaSuccess) st = RC_ERR_CUDA;
+            if (st == RC_SUCCESS) st = precond_on(R, n, Z, n, cs);
+            if (cudaStreamEndCapture(cs, &graph) != cudaSuccess && st == RC_SUCCESS) st = RC_ERR_CUDA;
+            cudaStreamDestroy(cs);
+            graph_kernels = (size_t)(rc_launch_count() - before);
+            if (st == RC_SUCCESS && cudaGraphInstantiate(&graph_exec, graph, 0) != cudaSuccess) st = RC_ERR_CUDA;
+            if (graph) cudaGraphDestroy(graph);
+            if (st != RC_SUCCESS) {
+                cudaGetLastError();
+                graph_exec = nullptr;
+                return st;
+            }
+        }
+        if (cudaGraphLaunch(graph_exec, s) != cudaSuccess) return RC_ERR_CUDA;
+        for (size_t i = 0; i < graph_kernels; ++i) count_launch();
+        return RC_SUCCESS;
+    }
+    ~Mixed() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
     }
 
     // Rout = B - A X (FP64, DMMA).
@@ -286,9 +321,11 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     if (o.tol <= 0) o.tol = 1e-15;
     if (o.max_iter < 0) o.max_iter = 100;
     const double uf = prec == RC_PREC_BF16 ? std::ldexp(1.0, -8) : std::ldexp(1.0, -11);
-    // shift_factor < 0: adaptive -- no shift first, then 1, 8, 64 u_f after a breakdown.
+    // shift_factor < 0: adaptive -- theta = u_f first (measured: a better preconditioner
+    // than no shift at kappa = 1e6, ~100 vs ~180-260 CG steps), then 8 and 64 u_f after a
+    // breakdown of the low-precision factorisation.
     const bool adaptive = o.shift_factor < 0.0;
-    double theta = adaptive ? 0.0 : o.shift_factor * uf;
+    double theta = adaptive ? uf : o.shift_factor * uf;
 
     size_t bytes = 0;
     mixed_workspace_bytes(n, nrhs, prec, o.outer, &bytes);
@@ -328,8 +365,8 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
         if (cudaMemcpyAsync(&h_info, d_info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess)
             return RC_ERR_CUDA;
-        if (h_info == 0 || !adaptive || attempt == 3) break;
-        theta = (attempt == 0 ? 1.0 : attempt == 1 ? 8.0 : 64.0) * uf;
+        if (h_info == 0 || !adaptive || attempt == 2) break;
+        theta = (attempt == 0 ? 8.0 : 64.0) * uf;
     }
     cudaEventRecord(e1, s);
     rc_refine_info info = {};
@@ -380,7 +417,7 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
             for (char d : done) all = all && d;
             if (all || iters >= o.max_iter) break;
             // (re)start CG from the true residual: Z = M^-1 R, P = Z, rz = R.Z
-            RC_TRY(M.precond(Rm, ldm, M.Z, ldm));
+            RC_TRY(M.precond_RZ());
             RC_TRY(copy2d<double, double>(n, nrhs, 1.0, View<const double>{M.Z, 1, ldm}, colmajor(M.P, ldm), s));
             RC_TRY(M.col_reduce(Rm, ldm, M.Z, ldm, 1, rz, M.dev_scalars));
             restart = false;
@@ -413,7 +450,7 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
             continue;
         }
         // Z = M^-1 R; beta = rz_new / rz; P = Z + beta P
-        RC_TRY(M.precond(Rm, ldm, M.Z, ldm));
+        RC_TRY(M.precond_RZ());
         std::vector<double> rz_new;
         RC_TRY(M.col_reduce(Rm, ldm, M.Z, ldm, 1, rz_new, M.dev_scalars));
         for (int64_t j = 0; j < nrhs; ++j) {
