@@ -1,0 +1,72 @@
+// remora/cuda/fwd.hpp -- the cuda_tag device and the declarations of its kernel overloads.
+//
+// Remora binds its kernel calls by qualified name inside templates
+// (e.g. kernels::gemm in detail/matrix_expression_classes.hpp:1004-1012,
+// bindings::matrix_assign in kernels/matrix_assign.hpp, bindings::generate_normal in
+// kernels/random.hpp:44-62), and qualified names are looked up where the template is
+// defined. So every cuda_tag overload is declared here, before remora.hpp is parsed;
+// remora/cuda.hpp includes this file first and the definitions after remora.hpp.
+#ifndef REMORA_CUDA_FWD_HPP
+#define REMORA_CUDA_FWD_HPP
+
+#include <cstddef>
+
+#include <remora/detail/traits.hpp>
+#include <remora/expression_types.hpp>
+
+namespace remora {
+
+/// \brief Device tag of the B200 (sm_100a) backend; joins cpu_tag, opencl_tag and hip_tag
+/// (expression_types.hpp:33-35).
+struct cuda_tag {};
+
+namespace cuda {
+class device;
+}
+
+namespace bindings {
+// Dense assignment X = E (X row-major after the dispatcher's transposition,
+// kernels/matrix_assign.hpp:76-105).
+template <class M, class E, class EOrientation, class TagE, class TagM>
+void matrix_assign(matrix_expression<M, cuda_tag>& m, matrix_expression<E, cuda_tag> const& e, row_major,
+                   EOrientation, TagE, TagM);
+
+// RNG fills, the hip_tag overloads of kernels/hip/random.hpp:261-323.
+template <class M, class Rng>
+void generate_normal(matrix_expression<M, cuda_tag>& m, Rng& rng, typename M::value_type mean,
+                     typename M::value_type variance);
+template <class M, class Rng>
+void generate_uniform(matrix_expression<M, cuda_tag>& m, Rng& rng, typename M::value_type low,
+                      typename M::value_type high);
+template <class M, class Rng>
+void generate_discrete(matrix_expression<M, cuda_tag>& m, Rng& rng, int low, int high);
+template <class V, class Rng>
+void generate_normal(vector_expression<V, cuda_tag>& v, Rng& rng, typename V::value_type mean,
+                     typename V::value_type variance);
+template <class V, class Rng>
+void generate_uniform(vector_expression<V, cuda_tag>& v, Rng& rng, typename V::value_type low,
+                      typename V::value_type high);
+template <class V, class Rng>
+void generate_discrete(vector_expression<V, cuda_tag>& v, Rng& rng, int low, int high);
+}  // namespace bindings
+
+namespace kernels {
+// C += alpha * A * B (kernels/gemm.hpp:85-106; hip: kernels/hip/gemm.hpp:90-112).
+template <class MatA, class MatB, class MatC>
+void gemm(matrix_expression<MatA, cuda_tag> const& A, matrix_expression<MatB, cuda_tag> const& B,
+          matrix_expression<MatC, cuda_tag>& C, typename MatC::value_type const& alpha);
+// Triangle of C += alpha * A * A^T (kernels/syrk.hpp:55-67; hip: kernels/hip/syrk.hpp:44-85).
+template <bool Upper, class MatA, class MatC>
+void syrk(matrix_expression<MatA, cuda_tag> const& A, matrix_expression<MatC, cuda_tag>& C,
+          typename MatC::value_type const& alpha);
+// B <- A^-1 B / B A^-1 (kernels/trsm.hpp:55-65; hip: kernels/hip/trsm.hpp:90-107).
+template <class Triangular, class Side, class MatA, class MatB>
+void trsm(matrix_expression<MatA, cuda_tag> const& A, matrix_expression<MatB, cuda_tag>& B);
+// In-place Cholesky (kernels/potrf.hpp:56-62; hip: kernels/hip/potrf.hpp:131-141).
+template <class Triangular, class MatA>
+std::size_t potrf(matrix_container<MatA, cuda_tag>& A);
+}  // namespace kernels
+
+}  // namespace remora
+
+#endif

@@ -1,0 +1,273 @@
+// remora/cuda/kernels.hpp -- definitions of the cuda_tag kernel overloads declared in
+// fwd.hpp. Each maps Remora's orientation-typed views onto the column-major C-ABI the
+// same way the reference's HIP backend maps them onto cuBLAS (a row-major matrix is the
+// transpose of a column-major one: kernels/hip/gemm.hpp:46-88, kernels/hip/syrk.hpp:
+// 61-67, kernels/hip/trsm.hpp:45-88) and enqueues on the result's device stream.
+#ifndef REMORA_CUDA_KERNELS_HPP
+#define REMORA_CUDA_KERNELS_HPP
+
+#include <cmath>
+#include <cstdint>
+#include <random>
+#include <type_traits>
+
+#include "dense.hpp"
+
+namespace remora {
+namespace cuda {
+namespace detail {
+
+template <class O>
+constexpr int trans_of() {  // 1 when a matrix of orientation O is the transpose of its column-major storage
+    return std::is_same<typename O::orientation, row_major>::value ? 1 : 0;
+}
+
+template <class T>
+struct blas;
+template <>
+struct blas<double> {
+    static int gemm(int ta, int tb, std::size_t m, std::size_t n, std::size_t k, double alpha, double const* A,
+                    std::size_t lda, double const* B, std::size_t ldb, double beta, double* C, std::size_t ldc,
+                    void* s) {
+        return rc_gemm_f64(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    }
+    static int syrk(int up, int t, std::size_t n, std::size_t k, double alpha, double const* A, std::size_t lda,
+                    double beta, double* C, std::size_t ldc, void* s) {
+        return rc_syrk_f64(up, t, n, k, alpha, A, lda, beta, C, ldc, s);
+    }
+    static int trsm(int left, int up, int t, int unit, std::size_t m, std::size_t n, double const* A, std::size_t lda,
+                    double* B, std::size_t ldb, void* s) {
+        return rc_trsm_f64(left, up, t, unit, m, n, 1.0, A, lda, B, ldb, nullptr, s);
+    }
+    static int potrf(int up, std::size_t n, double* A, std::size_t lda, int* info, void* s) {
+        return rc_potrf_f64(up, n, A, lda, info, s);
+    }
+};
+template <>
+struct blas<float> {
+    static int gemm(int ta, int tb, std::size_t m, std::size_t n, std::size_t k, float alpha, float const* A,
+                    std::size_t lda, float const* B, std::size_t ldb, float beta, float* C, std::size_t ldc,
+                    void* s) {
+        return rc_gemm_f32(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    }
+    static int syrk(int up, int t, std::size_t n, std::size_t k, float alpha, float const* A, std::size_t lda,
+                    float beta, float* C, std::size_t ldc, void* s) {
+        return rc_syrk_f32(up, t, n, k, alpha, A, lda, beta, C, ldc, s);
+    }
+    static int trsm(int left, int up, int t, int unit, std::size_t m, std::size_t n, float const* A, std::size_t lda,
+                    float* B, std::size_t ldb, void* s) {
+        return rc_trsm_f32(left, up, t, unit, m, n, 1.0f, A, lda, B, ldb, nullptr, s);
+    }
+    static int potrf(int up, std::size_t n, float* A, std::size_t lda, int* info, void* s) {
+        return rc_potrf_f32(up, n, A, lda, info, s);
+    }
+};
+
+/// Per-device status word for potrf (read back to return the pivot, as the reference does).
+inline int* status_word(device& dev) {
+    thread_local std::map<int, std::shared_ptr<void>> words;
+    auto& w = words[dev.id()];
+    if (!w) {
+        dev.set_device();
+        void* p = nullptr;
+        check(rc_malloc(&p, sizeof(int)), "rc_malloc");
+        w = std::shared_ptr<void>(p, [](void* q) { rc_free(q); });
+    }
+    return static_cast<int*>(w.get());
+}
+
+}  // namespace detail
+}  // namespace cuda
+
+namespace kernels {
+
+template <class MatA, class MatB, class MatC>
+void gemm(matrix_expression<MatA, cuda_tag> const& A, matrix_expression<MatB, cuda_tag> const& B,
+          matrix_expression<MatC, cuda_tag>& C, typename MatC::value_type const& alpha) {
+    REMORA_SIZE_CHECK(A().size1() == C().size1());
+    REMORA_SIZE_CHECK(B().size2() == C().size2());
+    REMORA_SIZE_CHECK(A().size2() == B().size1());
+    typedef typename MatC::value_type T;
+    static_assert(std::is_same<typename MatA::value_type, T>::value, "[gemm] Arguments do not have same element type");
+    static_assert(std::is_same<typename MatB::value_type, T>::value, "[gemm] Arguments do not have same element type");
+    auto const& Ae = eval_expression(A);
+    auto const& Be = eval_expression(B);
+    auto sa = Ae.raw_storage();
+    auto sb = Be.raw_storage();
+    auto sc = C().raw_storage();
+    const int ta = cuda::detail::trans_of<typename std::decay<decltype(Ae)>::type::orientation>();
+    const int tb = cuda::detail::trans_of<typename std::decay<decltype(Be)>::type::orientation>();
+    const int tc = cuda::detail::trans_of<typename MatC::orientation>();
+    const std::size_t m = C().size1(), n = C().size2(), k = A().size2();
+    void* s = C().queue().stream();
+    if (!tc)
+        cuda::check(cuda::detail::blas<T>::gemm(ta, tb, m, n, k, alpha, sa.values, sa.leading_dimension, sb.values,
+                                                sb.leading_dimension, T(1), sc.values, sc.leading_dimension, s),
+                    "rc_gemm");
+    else  // C^T = B^T A^T
+        cuda::check(cuda::detail::blas<T>::gemm(1 - tb, 1 - ta, n, m, k, alpha, sb.values, sb.leading_dimension,
+                                                sa.values, sa.leading_dimension, T(1), sc.values,
+                                                sc.leading_dimension, s),
+                    "rc_gemm");
+}
+
+template <bool Upper, class MatA, class MatC>
+void syrk(matrix_expression<MatA, cuda_tag> const& A, matrix_expression<MatC, cuda_tag>& C,
+          typename MatC::value_type const& alpha) {
+    REMORA_SIZE_CHECK(A().size1() == C().size1());
+    REMORA_SIZE_CHECK(C().size1() == C().size2());
+    typedef typename MatC::value_type T;
+    auto const& Ae = eval_expression(A);
+    auto sa = Ae.raw_storage();
+    auto sc = C().raw_storage();
+    const int ta = cuda::detail::trans_of<typename std::decay<decltype(Ae)>::type::orientation>();
+    const int tc = cuda::detail::trans_of<typename MatC::orientation>();
+    const int up = (Upper ? 1 : 0) ^ tc;  // a row-major C's upper triangle is its storage's lower one
+    cuda::check(cuda::detail::blas<T>::syrk(up, ta, C().size1(), A().size2(), alpha, sa.values, sa.leading_dimension,
+                                            T(1), sc.values, sc.leading_dimension, C().queue().stream()),
+                "rc_syrk");
+}
+
+template <class Triangular, class Side, class MatA, class MatB>
+void trsm(matrix_expression<MatA, cuda_tag> const& A, matrix_expression<MatB, cuda_tag>& B) {
+    REMORA_SIZE_CHECK(A().size1() == A().size2());
+    typedef typename MatB::value_type T;
+    auto const& Ae = eval_expression(A);
+    auto sa = Ae.raw_storage();
+    auto sb = B().raw_storage();
+    const int ta = cuda::detail::trans_of<typename std::decay<decltype(Ae)>::type::orientation>();
+    const int tb = cuda::detail::trans_of<typename MatB::orientation>();
+    const int up = (Triangular::is_upper ? 1 : 0) ^ ta;  // the triangle as stored
+    int left = Side::is_left ? 1 : 0, trans = ta;
+    std::size_t m = B().size1(), n = B().size2();
+    if (tb) {  // B row-major: solve for B^T on the other side with op(A)^T
+        left = 1 - left;
+        trans = 1 - ta;
+        std::swap(m, n);
+    }
+    cuda::check(cuda::detail::blas<T>::trsm(left, up, trans, Triangular::is_unit ? 1 : 0, m, n, sa.values,
+                                            sa.leading_dimension, sb.values, sb.leading_dimension,
+                                            B().queue().stream()),
+                "rc_trsm");
+}
+
+template <class Triangular, class MatA>
+std::size_t potrf(matrix_container<MatA, cuda_tag>& A) {
+    REMORA_SIZE_CHECK(A().size1() == A().size2());
+    typedef typename MatA::value_type T;
+    auto sa = A().raw_storage();
+    const int ta = cuda::detail::trans_of<typename MatA::orientation>();
+    cuda::device& dev = A().queue();
+    int* info = cuda::detail::status_word(dev);
+    cuda::check(cuda::detail::blas<T>::potrf((Triangular::is_upper ? 1 : 0) ^ ta, A().size1(), sa.values,
+                                             sa.leading_dimension, info, dev.stream()),
+                "rc_potrf");
+    int h = 0;
+    cuda::check(rc_memcpy2d(&h, sizeof(int), info, sizeof(int), sizeof(int), 1, RC_COPY_D2H, dev.stream()),
+                "rc_memcpy2d");
+    dev.synchronize();
+    return (std::size_t)h;  // 0, or the global 1-based index of the failing pivot
+}
+
+}  // namespace kernels
+
+namespace bindings {
+
+template <class M, class E, class EOrientation, class TagE, class TagM>
+void matrix_assign(matrix_expression<M, cuda_tag>& m, matrix_expression<E, cuda_tag> const& e, row_major,
+                   EOrientation, TagE, TagM) {
+    typedef typename M::value_type T;
+    auto const& Ee = eval_expression(e);
+    auto se = Ee.raw_storage();
+    auto sm = m().raw_storage();
+    // m is row-major: its storage is the column-major size2 x size1 matrix m^T.
+    const int te = cuda::detail::trans_of<typename std::decay<decltype(Ee)>::type::orientation>();
+    cuda::check(cuda::detail::abi<T>::copy(te ? 0 : 1, m().size2(), m().size1(), T(1), se.values, se.leading_dimension,
+                                           sm.values, sm.leading_dimension, m().queue().stream()),
+                "rc_copy2d");
+}
+
+namespace cuda_detail {
+template <class Rng>
+void draw_key(Rng& rng, std::uint32_t key[4]) {
+    // kernels/hip/random.hpp:225-227
+    std::uniform_int_distribution<std::uint32_t> dist(0, 0xffffffff);
+    for (int i = 0; i != 4; ++i) key[i] = dist(rng);
+}
+template <class M>
+void fill_args(M const& m, float*& p, std::size_t& ld, int& row) {
+    static_assert(std::is_same<typename M::value_type, float>::value,
+                  "only 32 bit random number types are supported (as kernels/hip/random.hpp:222)");
+    auto s = m.raw_storage();
+    p = s.values;
+    ld = s.leading_dimension;
+    row = cuda::detail::trans_of<typename M::orientation>();
+}
+}  // namespace cuda_detail
+
+template <class M, class Rng>
+void generate_normal(matrix_expression<M, cuda_tag>& m, Rng& rng, typename M::value_type mean,
+                     typename M::value_type variance) {
+    std::uint32_t key[4];
+    cuda_detail::draw_key(rng, key);
+    float* p; std::size_t ld; int row;
+    cuda_detail::fill_args(m(), p, ld, row);
+    cuda::check(rc_rng_normal_f32(key, m().size1(), m().size2(), p, ld, row, mean, std::sqrt(variance),
+                                  m().queue().stream()),
+                "rc_rng_normal_f32");
+}
+template <class M, class Rng>
+void generate_uniform(matrix_expression<M, cuda_tag>& m, Rng& rng, typename M::value_type low,
+                      typename M::value_type high) {
+    std::uint32_t key[4];
+    cuda_detail::draw_key(rng, key);
+    float* p; std::size_t ld; int row;
+    cuda_detail::fill_args(m(), p, ld, row);
+    cuda::check(rc_rng_uniform_f32(key, m().size1(), m().size2(), p, ld, row, low, high, m().queue().stream()),
+                "rc_rng_uniform_f32");
+}
+template <class M, class Rng>
+void generate_discrete(matrix_expression<M, cuda_tag>& m, Rng& rng, int low, int high) {
+    std::uint32_t key[4];
+    cuda_detail::draw_key(rng, key);
+    float* p; std::size_t ld; int row;
+    cuda_detail::fill_args(m(), p, ld, row);
+    cuda::check(rc_rng_discrete_f32(key, m().size1(), m().size2(), p, ld, row, low, high, m().queue().stream()),
+                "rc_rng_discrete_f32");
+}
+// A vector is filled as a 1 x n row-major matrix (kernels/hip/random.hpp:269).
+template <class V, class Rng>
+void generate_normal(vector_expression<V, cuda_tag>& v, Rng& rng, typename V::value_type mean,
+                     typename V::value_type variance) {
+    static_assert(std::is_same<typename V::value_type, float>::value, "only 32 bit random number types");
+    std::uint32_t key[4];
+    cuda_detail::draw_key(rng, key);
+    auto s = v().raw_storage();
+    cuda::check(rc_rng_normal_f32(key, 1, v().size(), s.values, v().size(), 1, mean, std::sqrt(variance),
+                                  v().queue().stream()),
+                "rc_rng_normal_f32");
+}
+template <class V, class Rng>
+void generate_uniform(vector_expression<V, cuda_tag>& v, Rng& rng, typename V::value_type low,
+                      typename V::value_type high) {
+    static_assert(std::is_same<typename V::value_type, float>::value, "only 32 bit random number types");
+    std::uint32_t key[4];
+    cuda_detail::draw_key(rng, key);
+    auto s = v().raw_storage();
+    cuda::check(rc_rng_uniform_f32(key, 1, v().size(), s.values, v().size(), 1, low, high, v().queue().stream()),
+                "rc_rng_uniform_f32");
+}
+template <class V, class Rng>
+void generate_discrete(vector_expression<V, cuda_tag>& v, Rng& rng, int low, int high) {
+    static_assert(std::is_same<typename V::value_type, float>::value, "only 32 bit random number types");
+    std::uint32_t key[4];
+    cuda_detail::draw_key(rng, key);
+    auto s = v().raw_storage();
+    cuda::check(rc_rng_discrete_f32(key, 1, v().size(), s.values, v().size(), 1, low, high, v().queue().stream()),
+                "rc_rng_discrete_f32");
+}
+
+}  // namespace bindings
+}  // namespace remora
+
+#endif

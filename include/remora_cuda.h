@@ -54,6 +54,25 @@ int rc_device_status(void* stream);
 int rc_selftest_wait_timeout(uint64_t limit_ns, void* stream);
 
 /* ---------------------------------------------------------------------------------
+ * Device runtime for hosts compiled without the CUDA toolkit (the cuda_tag headers).
+ * Replace the HIP runtime plumbing of include/remora/hip/device.hpp:41-180 (device,
+ * stream per thread), include/remora/hip/buffer.hpp:41-102 (owning allocation) and the
+ * transport of include/remora/hip/copy.hpp:131-410 (here: pitched asynchronous copies;
+ * host memory need not be pinned, in which case the copy is synchronous). */
+enum { RC_COPY_H2D = 1, RC_COPY_D2H = 2, RC_COPY_D2D = 3 };
+int rc_device_count(int* count);
+int rc_set_device(int device);
+int rc_get_device(int* device);
+int rc_malloc(void** ptr, size_t bytes);
+int rc_free(void* ptr);
+/* Copy `rows` rows of width_bytes bytes; row r of src starts at src + r * spitch. */
+int rc_memcpy2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width_bytes,
+                size_t rows, int kind, void* stream);
+int rc_stream_create(void** stream);
+int rc_stream_destroy(void* stream);
+int rc_stream_synchronize(void* stream);
+
+/* ---------------------------------------------------------------------------------
  * Counter-based RNG fills of a rows x cols float/int matrix (Threefry-4x32, 12 rounds).
  * Replaces bindings::generate_normal/uniform/discrete for hip_tag,
  * include/remora/kernels/hip/random.hpp:218-323 (kernels :163-210, generator :40-161).

@@ -38,6 +38,15 @@ SIGNATURES: dict[str, list] = {
     "rc_error_string": [_I],
     "rc_release_workspaces": [],
     "rc_launch_count": [],
+    "rc_device_count": [_P],
+    "rc_set_device": [_I],
+    "rc_get_device": [_P],
+    "rc_malloc": [_P, _Z],
+    "rc_free": [_P],
+    "rc_memcpy2d": [_P, _Z, _P, _Z, _Z, _Z, _I, _P],
+    "rc_stream_create": [_P],
+    "rc_stream_destroy": [_P],
+    "rc_stream_synchronize": [_P],
     "rc_rng_bits_u32": [_U4, _Z, _Z, _P, _Z, _I, _P],
     "rc_rng_uniform_f32": [_U4, _Z, _Z, _P, _Z, _I, c_float, c_float, _P],
     "rc_rng_normal_f32": [_U4, _Z, _Z, _P, _Z, _I, c_float, c_float, _P],
