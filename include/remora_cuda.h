@@ -167,6 +167,22 @@ int rc_spd_solve_f64_noalloc(size_t n, size_t nrhs, const double* A, size_t lda,
                              size_t ldb, int* d_info, void* stream);
 
 /* ---------------------------------------------------------------------------------
+ * Batched uneven SPD solves (extension; the reference solves one system per
+ * cholesky_decomposition, decompositions.hpp:81-115). System i: the n_i x n_i SPD matrix
+ * at d_A[i] (column-major, ld = n_i, lower triangle read, overwritten by its Cholesky
+ * factor) and the right-hand side at d_b[i] (overwritten by the solution);
+ * 1 <= n_i <= 512. d_A and d_b are DEVICE arrays of device pointers, h_n a HOST array of
+ * sizes, d_info a device array receiving 0 or each system's failing pivot (1-based).
+ * One persistent launch replayed as a CUDA graph; the graph and the tile configuration
+ * (autotune = 1: timed on this batch the first time, cached per precision and size
+ * bucket) are kept per (device, d_A, d_b, d_info, count) until rc_batched_release_plans. */
+int rc_potrf_trsm_batched_f64(size_t count, const int* h_n, double* const* d_A, double* const* d_b,
+                              int* d_info, int autotune, void* stream);
+int rc_potrf_trsm_batched_f32(size_t count, const int* h_n, float* const* d_A, float* const* d_b,
+                              int* d_info, int autotune, void* stream);
+int rc_batched_release_plans(void);
+
+/* ---------------------------------------------------------------------------------
  * Mixed-precision refined SPD solve (extension; no reference counterpart -- the reference
  * solves SPD systems only in the working precision, decompositions.hpp:81-105).
  * X = A^-1 B for a symmetric positive definite A given in FULL (both triangles), FP64:

@@ -67,6 +67,9 @@ SIGNATURES: dict[str, list] = {
     "rc_potrf_f32": [_I, _Z, _P, _Z, _P, _P],
     "rc_spd_solve_f64": [_Z, _Z, _P, _Z, _P, _Z, _P, _P],
     "rc_spd_solve_f64_noalloc": [_Z, _Z, _P, _Z, _P, _Z, _P, _P],
+    "rc_potrf_trsm_batched_f64": [_Z, _P, _P, _P, _P, _I, _P],
+    "rc_potrf_trsm_batched_f32": [_Z, _P, _P, _P, _P, _I, _P],
+    "rc_batched_release_plans": [],
     "rc_spd_solve_mixed": [_I, _Z, _Z, _P, _Z, _P, _Z, _P, _Z, _P, _P, _P, _P],
     "rc_spd_solve_mixed_workspace": [_I, _Z, _Z, _P, _P],
     "rc_syrk_tc": [_I, _Z, _Z, c_float, _P, _Z, c_float, _P, _Z, _P],

@@ -189,3 +189,44 @@ def spd_solve_mixed(A: torch.Tensor, B: torch.Tensor, precision: str = "tf32", t
     out = {f: getattr(info, f) for f, _ in RefineInfo._fields_}
     out["pivot"] = int(d_info.item())
     return X, out, status
+
+
+class BatchedSystems:
+    """Device storage for a batch of uneven SPD systems (one RHS each) laid out as
+    consecutive column-major blocks, with the pointer arrays the batched C-ABI takes."""
+
+    def __init__(self, mats, rhs, dtype=torch.float64, device="cuda"):
+        import numpy as np
+        self.sizes = np.array([m.shape[0] for m in mats], dtype=np.int32)
+        offs = np.concatenate([[0], np.cumsum(self.sizes.astype(np.int64) ** 2)])
+        self.A = torch.empty(int(offs[-1]), dtype=dtype, device=device)
+        boffs = np.concatenate([[0], np.cumsum(self.sizes.astype(np.int64))])
+        self.b = torch.empty(int(boffs[-1]), dtype=dtype, device=device)
+        host_a = np.concatenate([np.asarray(m, dtype=np.float64).T.reshape(-1) for m in mats])  # column-major
+        host_b = np.concatenate([np.asarray(v, dtype=np.float64).reshape(-1) for v in rhs])
+        self.A.copy_(torch.from_numpy(host_a))
+        self.b.copy_(torch.from_numpy(host_b))
+        es = self.A.element_size()
+        self.a_ptrs = torch.tensor([self.A.data_ptr() + int(o) * es for o in offs[:-1]], dtype=torch.int64,
+                                   device=device)
+        self.b_ptrs = torch.tensor([self.b.data_ptr() + int(o) * es for o in boffs[:-1]], dtype=torch.int64,
+                                   device=device)
+        self.info = torch.zeros(len(mats), dtype=torch.int32, device=device)
+        self.offs, self.boffs = offs, boffs
+
+    def solve(self, autotune: bool = True) -> None:
+        from ._lib import lib
+        fn = "rc_potrf_trsm_batched_f64" if self.A.dtype == torch.float64 else "rc_potrf_trsm_batched_f32"
+        sizes = self.sizes.ctypes.data_as(ctypes.c_void_p)
+        status = getattr(lib(), fn)(len(self.sizes), sizes, _ptr(self.a_ptrs), _ptr(self.b_ptrs), _ptr(self.info),
+                                    int(autotune), _stream())
+        if status != 0:
+            from ._lib import RemoraCudaError
+            raise RemoraCudaError(fn, status)
+
+    def factor(self, i: int):
+        n = int(self.sizes[i])
+        return self.A[int(self.offs[i]):int(self.offs[i + 1])].view(n, n).t()  # column-major n x n
+
+    def solution(self, i: int):
+        return self.b[int(self.boffs[i]):int(self.boffs[i + 1])]
