@@ -229,6 +229,31 @@ int rc_spd_solve_mixed_workspace(int precision, size_t n, size_t nrhs,
                                  const rc_mixed_options* options, size_t* bytes);
 
 /* ---------------------------------------------------------------------------------
+ * Reverse-mode adjoints (extension; the reference has no derivatives of its
+ * decompositions). Column-major FP64, device pointers.
+ * rc_potrf_backward_f64: for A = L L^T (L lower, e.g. from rc_potrf_f64; only its lower
+ *   triangle is read) and the adjoint Lbar of L (lower triangle read), writes the full
+ *   symmetric adjoint Abar = 1/2 L^-T (P + P^T) L^-1, P = Phi(L^T Lbar) (Murray 2016),
+ *   computed from L alone with blocked GEMM/TRSM kernels.
+ * rc_trsm_backward_f64: reverse mode of X = L^-1 B (trans = 0) or X = L^-T B (trans = 1)
+ *   with n x nrhs X: Xbar is overwritten by Bbar, and the lower triangle of Lbar
+ *   accumulates -tril(Bbar X^T) (trans = 0) or -tril(X Bbar^T) (trans = 1). */
+int rc_potrf_backward_f64(size_t n, const double* L, size_t ldl, const double* Lbar, size_t ldlb,
+                          double* Abar, size_t ldab, void* stream);
+int rc_trsm_backward_f64(int trans, size_t n, size_t nrhs, const double* L, size_t ldl,
+                         const double* X, size_t ldx, double* Xbar, size_t ldxb, double* Lbar,
+                         size_t ldlb, void* stream);
+/* Gaussian-process RBF kernel around the differentiated Cholesky: X is n x d row-major
+ * (d <= 16), ls the d lengthscales. rc_rbf_kernel_f64 writes
+ * K_ij = exp(-1/2 sum_q ((x_iq - x_jq) / ls_q)^2) + noise [i == j]; the gradient call
+ * writes grad_q = sum_ij Kbar_ij k_ij (x_iq - x_jq)^2 / ls_q^3 (the chain rule from the
+ * adjoint Kbar of K to the lengthscales). */
+int rc_rbf_kernel_f64(size_t n, int d, const double* X, const double* ls, double noise, double* K,
+                      size_t ldk, void* stream);
+int rc_rbf_lengthscale_grad_f64(size_t n, int d, const double* X, const double* ls,
+                                const double* Kbar, size_t ldk, double* grad, void* stream);
+
+/* ---------------------------------------------------------------------------------
  * Assignment support for the containers (include/remora/kernels/hip/matrix_assign.hpp:
  * 38-200, include/remora/hip/dense.hpp:39-51, hip/buffer.hpp:105-125).
  * rc_copy2d_*: B <- alpha * op(A) (A m x n if !trans, n x m if trans; B m x n).

@@ -230,3 +230,60 @@ class BatchedSystems:
 
     def solution(self, i: int):
         return self.b[int(self.boffs[i]):int(self.boffs[i + 1])]
+
+
+def potrf_backward(L: torch.Tensor, Lbar: torch.Tensor, Abar: torch.Tensor | None = None) -> torch.Tensor:
+    """Adjoint of A = L L^T: the full symmetric Abar for the adjoint Lbar of the lower L
+    (column-major FP64)."""
+    n = L.shape[0]
+    if Abar is None:
+        Abar = torch.empty((n, n), dtype=torch.float64, device=L.device).t()
+    _, ldl = layout(L)
+    _, ldlb = layout(Lbar)
+    _, ldab = layout(Abar)
+    call("rc_potrf_backward_f64", n, _ptr(L), ldl, _ptr(Lbar), ldlb, _ptr(Abar), ldab, _stream())
+    return Abar
+
+
+def trsm_backward(L: torch.Tensor, X: torch.Tensor, Xbar: torch.Tensor, Lbar: torch.Tensor,
+                  trans: bool = False) -> torch.Tensor:
+    """Reverse mode of X = L^-1 B (trans: X = L^-T B): Xbar becomes Bbar (returned), Lbar
+    accumulates the adjoint of L."""
+    n, nrhs = X.shape
+    call("rc_trsm_backward_f64", int(trans), n, nrhs, _ptr(L), layout(L)[1], _ptr(X), layout(X)[1], _ptr(Xbar),
+         layout(Xbar)[1], _ptr(Lbar), layout(Lbar)[1], _stream())
+    return Xbar
+
+
+def rbf_kernel(X: torch.Tensor, ls: torch.Tensor, noise: float) -> torch.Tensor:
+    n, d = X.shape
+    K = torch.empty((n, n), dtype=torch.float64, device=X.device).t()
+    call("rc_rbf_kernel_f64", n, d, _ptr(X.contiguous()), _ptr(ls), noise, _ptr(K), n, _stream())
+    return K
+
+
+def gp_nll_and_grad(X: torch.Tensor, y: torch.Tensor, ls: torch.Tensor, noise: float):
+    """Negative log marginal likelihood of a GP with an RBF kernel (constant term
+    dropped), f = 1/2 y^T K^-1 y + 1/2 log det K, and df/dls, all through the C-ABI:
+    forward Cholesky + triangular solve, backward through the hand-written TRSM and
+    Cholesky adjoints, then the lengthscale contraction."""
+    n, d = X.shape
+    Xc = X.contiguous()
+    K = rbf_kernel(Xc, ls, noise)
+    L = K.clone()
+    info = potrf(L)
+    if info:
+        raise RuntimeError(f"K is not positive definite (pivot {info})")
+    z = y.reshape(n, 1).clone().t().contiguous().t()
+    trsm(L, z)  # z = L^-1 y
+    Ld = torch.diagonal(L)
+    f = 0.5 * float((z * z).sum()) + float(torch.log(Ld).sum())
+    # backward: zbar = z; through z = L^-1 y; then d(sum log L_ii)/dL_ii = 1/L_ii
+    Lbar = torch.zeros((n, n), dtype=torch.float64, device=X.device).t()
+    zbar = z.clone()
+    trsm_backward(L, z, zbar, Lbar, trans=False)
+    Lbar.diagonal().add_(1.0 / Ld)
+    Kbar = potrf_backward(L, Lbar)
+    g = torch.empty(d, dtype=torch.float64, device=X.device)
+    call("rc_rbf_lengthscale_grad_f64", n, d, _ptr(Xc), _ptr(ls), _ptr(Kbar), layout(Kbar)[1], _ptr(g), _stream())
+    return f, g, Kbar
