@@ -171,6 +171,43 @@ std::size_t potrf(matrix_container<MatA, cuda_tag>& A) {
 
 }  // namespace kernels
 
+namespace cuda {
+
+/// Reverse mode of A = L L^T: the full symmetric adjoint Abar of A for the adjoint Lbar
+/// of the lower factor L (all FP64, column-major, on the device). No reference
+/// counterpart; see rc_potrf_backward_f64.
+template <class ML, class MLb, class MAb>
+void potrf_backward(matrix_expression<ML, cuda_tag> const& L, matrix_expression<MLb, cuda_tag> const& Lbar,
+                    matrix_expression<MAb, cuda_tag>& Abar) {
+    static_assert(std::is_same<typename MAb::orientation::orientation, column_major>::value &&
+                      std::is_same<typename ML::orientation::orientation, column_major>::value &&
+                      std::is_same<typename MLb::orientation::orientation, column_major>::value,
+                  "potrf_backward takes column-major matrices");
+    auto sl = L().raw_storage();
+    auto slb = Lbar().raw_storage();
+    auto sa = Abar().raw_storage();
+    check(rc_potrf_backward_f64(L().size1(), sl.values, sl.leading_dimension, slb.values, slb.leading_dimension,
+                                sa.values, sa.leading_dimension, Abar().queue().stream()),
+          "rc_potrf_backward_f64");
+}
+
+/// Reverse mode of X = L^-1 B (trans = false) or X = L^-T B (trans = true): Xbar is
+/// overwritten by Bbar and the lower triangle of Lbar accumulates the adjoint of L.
+template <class ML, class MX, class MXb, class MLb>
+void trsm_backward(bool trans, matrix_expression<ML, cuda_tag> const& L, matrix_expression<MX, cuda_tag> const& X,
+                   matrix_expression<MXb, cuda_tag>& Xbar, matrix_expression<MLb, cuda_tag>& Lbar) {
+    auto sl = L().raw_storage();
+    auto sx = X().raw_storage();
+    auto sxb = Xbar().raw_storage();
+    auto slb = Lbar().raw_storage();
+    check(rc_trsm_backward_f64(trans ? 1 : 0, X().size1(), X().size2(), sl.values, sl.leading_dimension, sx.values,
+                               sx.leading_dimension, sxb.values, sxb.leading_dimension, slb.values,
+                               slb.leading_dimension, Lbar().queue().stream()),
+          "rc_trsm_backward_f64");
+}
+
+}  // namespace cuda
+
 namespace bindings {
 
 template <class M, class E, class EOrientation, class TagE, class TagM>

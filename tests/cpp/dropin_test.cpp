@@ -206,6 +206,45 @@ int main() {
         report("normal(g, r, c, 1, 4, cuda_tag()): |mean - 1|", std::fabs(mean - 1.0), 0.02);
         report("  ... |variance - 4|", std::fabs(var - 4.0), 0.05);
     }
+    // --- reverse mode: GP negative log likelihood f = 1/2 y^T K^-1 y + 1/2 log det K.
+    // Device: forward Cholesky + triangular solve, backward through the hand-written
+    // adjoints. Reference: Kbar = 1/2 (inv(K, symm_pos_def()) - alpha alpha^T) composed
+    // from Remora's CPU kernels (solve.hpp:472-493).
+    {
+        std::size_t n = 160;
+        std::mt19937 g(5);
+        matrix<double> X(n, 16);
+        vector<double> ydat(n);
+        kernels::generate_normal(X, g, 0.0, 1.0);
+        kernels::generate_normal(ydat, g, 0.0, 1.0);
+        matrix<double> K(n, n);
+        for (std::size_t i = 0; i != n; ++i)
+            for (std::size_t j = 0; j != n; ++j) {
+                double r2 = 0;
+                for (std::size_t q = 0; q != 16; ++q) r2 += (X(i, q) - X(j, q)) * (X(i, q) - X(j, q));
+                K(i, j) = std::exp(-0.5 * r2 / 4.0) + (i == j ? 1e-2 : 0.0);
+            }
+        matrix<double> y(n, 1);
+        for (std::size_t i = 0; i != n; ++i) y(i, 0) = ydat(i);
+        matrix<double, column_major, cuda_tag> L = copy_to_device(K, cuda_tag());
+        kernels::potrf<lower>(L);
+        matrix<double, column_major, cuda_tag> z = copy_to_device(y, cuda_tag());
+        kernels::trsm<lower, left>(L, z);  // z = L^-1 y
+        matrix<double> Lh = copy_to_cpu(L), zh = copy_to_cpu(z);
+        matrix<double, column_major, cuda_tag> zbar = z;  // d(1/2 z^T z)/dz = z
+        matrix<double> Lbar0(n, n, 0.0);
+        for (std::size_t i = 0; i != n; ++i) Lbar0(i, i) = 1.0 / Lh(i, i);  // d(sum log L_ii)/dL_ii
+        matrix<double, column_major, cuda_tag> Lbar = copy_to_device(Lbar0, cuda_tag());
+        cuda::trsm_backward(false, L, z, zbar, Lbar);
+        matrix<double, column_major, cuda_tag> Kbar(n, n);
+        cuda::potrf_backward(L, Lbar, Kbar);
+        matrix<double> Kinv = inv(K, symm_pos_def());
+        matrix<double> alpha = solve(K, y, symm_pos_def(), left());
+        matrix<double> ref = Kinv - prod(alpha, trans(alpha));
+        ref *= 0.5;
+        report("GP NLL adjoint dF/dK vs Remora CPU 1/2(inv(K) - a a^T)", rel_diff(matrix<double>(copy_to_cpu(Kbar)), ref),
+               1e-9);
+    }
     std::printf("%s (%d failures)\n", failures ? "FAILED" : "PASSED", failures);
     return failures ? 1 : 0;
 }
