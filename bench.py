@@ -348,6 +348,67 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def run_case(args) -> None:
+    """One small case of one kernel, repeated (warm-up + steps): the command the ncu
+    captures under profiles/ run. Inputs are larger than L2 where the kernel streams."""
+    import torch
+    from remora_b200 import _lib, ops
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    sptr = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    reps = args.warmup + args.steps
+    if args.case == "syrk_tc":  # the mixed factorisation's trailing update, n x n lower, depth 1024
+        n, k = 8192, 1024
+        P = torch.randn((n, k), device=dev, dtype=torch.float32)
+        if args.precision == "bf16":
+            P = P.bfloat16()
+        C = torch.zeros((n, n), device=dev, dtype=torch.float32)
+        for _ in range(reps):
+            _lib.call("rc_syrk_tc", 1 if args.precision == "bf16" else 0, n, k, -1.0, ctypes.c_void_p(P.data_ptr()),
+                      k, 1.0, ctypes.c_void_p(C.data_ptr()), n, sptr)
+    elif args.case == "dgemm":  # FP64 DMMA GEMM 4096^3
+        n = 4096
+        A = torch.rand((n, n), device=dev, dtype=torch.float64)
+        B = torch.rand((n, n), device=dev, dtype=torch.float64)
+        C = torch.zeros((n, n), device=dev, dtype=torch.float64)
+        for _ in range(reps):
+            ops.gemm(A, B, C, 1.0, 0.0)
+    elif args.case == "potrf":  # FP64 blocked Cholesky n = 8192 (diagonal blocks, panels, updates)
+        n = 8192
+        G = torch.randn((n, n), device=dev, dtype=torch.float64)
+        S = G @ G.T / n + torch.eye(n, device=dev, dtype=torch.float64)
+        W = torch.empty_like(S)
+        for _ in range(reps):
+            W.copy_(S)
+            ops.potrf(W, sync=False)
+    elif args.case == "rng":  # normal fill of 2^28 floats, 16384 x 16384 row-major
+        X = torch.empty((16384, 16384), device=dev, dtype=torch.float32)
+        for _ in range(reps):
+            ops.generate_normal(X, [1, 2, 3, 4], 0.0, 1.0)
+    elif args.case == "mixed":  # the headline solve at a reduced size
+        A = make_spd(args.n, args.kappa, seed=1234, device=dev)
+        B = torch.randn((args.nrhs, args.n), device=dev, dtype=torch.float64).t()
+        for _ in range(reps):
+            ops.spd_solve_mixed(A, B, args.precision, tol=1e-15, max_iter=args.max_iter)
+    elif args.case == "batched":  # 4096 uneven RBF systems, n ~ U{16..512}
+        import numpy as np
+        rs = np.random.default_rng(1)
+        mats, rhs = [], []
+        for n in rs.integers(16, 513, 4096):
+            X = rs.standard_normal((n, 8))
+            d2 = ((X[:, None, :] - X[None, :, :]) ** 2).sum(-1)
+            mats.append(np.exp(-0.5 * d2) + 1e-2 * np.eye(n))
+            rhs.append(rs.standard_normal(n))
+        sysb = ops.BatchedSystems(mats, rhs)
+        a0, b0 = sysb.A.clone(), sysb.b.clone()
+        for _ in range(reps):
+            sysb.A.copy_(a0)
+            sysb.b.copy_(b0)
+            sysb.solve()
+    torch.cuda.synchronize()
+    print(json.dumps({"case": args.case, "reps": reps, "ok": True}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -362,8 +423,12 @@ def main() -> None:
     ap.add_argument("--ref-n", type=int, default=4096, help="CPU reference sample size")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--case", choices=["syrk_tc", "dgemm", "potrf", "rng", "mixed", "batched"],
+                    help="run one small kernel case (for ncu captures) instead of the benchmark")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.case:
+        run_case(args)
+    elif args.impl == "reference":
         run_reference_arm(args)
     else:
         run_ours(args)
