@@ -126,12 +126,13 @@ __global__ void __launch_bounds__(256, 1) potrf_diag(View<T> A, int sz, int64_t 
                 return;
             }
             if (tx == jj) {
+                const double rsq = 1.0 / sq;  // one division per column, then products
 #pragma unroll
                 for (int r = 0; r < 8; ++r) {
                     const int i = ty + 16 * r;
                     double v = 0.0;
                     if (i == j) v = sq;
-                    else if (i > j) v = a[r][q] / sq;
+                    else if (i > j) v = a[r][q] * rsq;
                     if (i >= j) a[r][q] = v;
                     col[i] = v;
                 }

@@ -135,6 +135,138 @@ __global__ void from_f32_scaled_kernel(int64_t n, int64_t c, const double* s, co
             Z[i + j * ldz] = s[i] * (double)T[i + j * n];
 }
 
+// ---------------------------------------------------------------------------------------
+// Few-right-hand-side triangular solves with the FP32 factor (the CG preconditioner).
+// L is the row-major lower factor (ldw), Winv the row-major inverses of its kNB x kNB
+// diagonal blocks, right-hand sides column-major n x c (c <= 64, ld n). One block step
+// is two launches with every operand resident in shared memory (no k-loop barriers):
+//   diag:   X_b = M_b R_b          M_b = inv(L_bb) (forward) or inv(L_bb)^T (backward)
+//   update: forward  R[r0+sz:]  -= L[r0+sz:, r0:r0+sz] X_b
+//           backward R[:r0]     -= L[r0:r0+sz, :r0]^T   X_b
+constexpr int RHS = 64;
+constexpr int DP = kNB + 1;  // padded pitch of the inverse block in shared memory
+
+template <bool BWD>
+__global__ void __launch_bounds__(256) pre_diag_kernel(int64_t n, int c, int64_t r0, int sz, const float* Winv_b,
+                                                       const float* R, float* X) {
+    extern __shared__ float sm[];
+    float* M = sm;                  // kNB x DP: M[i * DP + k] = M_b(i, k)
+    float* Rb = sm + kNB * DP;      // kNB x RHS: Rb[k * RHS + j]
+    const int tid = threadIdx.x;
+    for (int e = tid; e < kNB * kNB; e += 256) {
+        const int a = e / kNB, b = e % kNB;  // Winv_b[a][b], coalesced
+        const float v = (a < sz && b < sz) ? Winv_b[e] : 0.f;
+        if (BWD) M[b * DP + a] = v; else M[a * DP + b] = v;
+    }
+    for (int e = tid; e < kNB * RHS; e += 256) {
+        const int k = e % kNB, j = e / kNB;  // column j, row k: coalesced along k
+        Rb[k * RHS + j] = (k < sz && j < c) ? R[(r0 + k) + (int64_t)j * n] : 0.f;
+    }
+    __syncthreads();
+    const int i = tid % kNB, j0 = (tid / kNB) * 32;
+    float acc[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) acc[q] = 0.f;
+    for (int k = 0; k < kNB; ++k) {
+        const float m = M[i * DP + k];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) acc[q] = fmaf(m, Rb[k * RHS + j0 + q], acc[q]);
+    }
+    if (i < sz)
+#pragma unroll
+        for (int q = 0; q < 32; ++q)
+            if (j0 + q < c) X[(r0 + i) + (int64_t)(j0 + q) * n] = acc[q];
+}
+
+// Rows [i0, i0 + 64) of R -= A_tile (64 x sz) * X_b (sz x c), A_tile from the factor.
+template <bool BWD>
+__global__ void __launch_bounds__(256) pre_update_kernel(int64_t n, int c, int64_t r0, int sz, int64_t row_begin,
+                                                         int64_t row_end, const float* W, int64_t ldw,
+                                                         const float* X, float* R) {
+    constexpr int AP = 64 + 4;  // pitch of As[k][i]
+    extern __shared__ float sm[];
+    float* As = sm;               // kNB x AP
+    float* Xs = sm + kNB * AP;    // kNB x RHS
+    const int tid = threadIdx.x;
+    const int64_t i0 = row_begin + (int64_t)blockIdx.x * 64;
+    for (int e = tid; e < 64 * kNB; e += 256) {
+        int ii, k;
+        float v = 0.f;
+        if (!BWD) {  // A(i, k) = L(i, r0 + k): row i of L is contiguous in k
+            ii = e / kNB; k = e % kNB;
+            const int64_t gi = i0 + ii;
+            if (gi < row_end && k < sz) v = W[gi * ldw + r0 + k];
+        } else {     // A(i, k) = L(r0 + k, i): row r0 + k of L is contiguous in i
+            k = e / 64; ii = e % 64;
+            const int64_t gi = i0 + ii;
+            if (gi < row_end && k < sz) v = W[(r0 + k) * ldw + gi];
+        }
+        As[k * AP + ii] = v;
+    }
+    for (int e = tid; e < kNB * RHS; e += 256) {
+        const int k = e % kNB, j = e / kNB;
+        Xs[k * RHS + j] = (k < sz && j < c) ? X[(r0 + k) + (int64_t)j * n] : 0.f;
+    }
+    __syncthreads();
+    const int tr = tid / 16, tc = tid % 16;
+    float acc[4][4] = {};
+    for (int k = 0; k < sz; ++k) {
+        const float4 a = *reinterpret_cast<const float4*>(As + k * AP + 4 * tr);
+        const float4 x = *reinterpret_cast<const float4*>(Xs + k * RHS + 4 * tc);
+        const float av[4] = {a.x, a.y, a.z, a.w}, xv[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], xv[v], acc[u][v]);
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const int j = 4 * tc + v;
+        if (j >= c) continue;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t gi = i0 + 4 * tr + u;
+            if (gi < row_end) R[gi + (int64_t)j * n] -= acc[u][v];
+        }
+    }
+}
+
+constexpr size_t kPreDiagSmem = (size_t)(kNB * DP + kNB * RHS) * sizeof(float);
+constexpr size_t kPreUpdSmem = (size_t)(kNB * (64 + 4) + kNB * RHS) * sizeof(float);
+
+// Solve L X = R (bwd = false) or L^T X = R (bwd = true) for c <= 64 columns; R is
+// consumed (updated in place), X receives the solution.
+int trsm_few(bool bwd, int64_t n, int c, const float* W, int64_t ldw, const float* Winv, float* R, float* X,
+             cudaStream_t st) {
+    const int64_t nblk = (n + kNB - 1) / kNB;
+    for (int64_t step = 0; step < nblk; ++step) {
+        const int64_t b = bwd ? nblk - 1 - step : step;
+        const int64_t r0 = b * kNB;
+        const int sz = (int)((n - r0) < kNB ? n - r0 : kNB);
+        const float* Wb = Winv + (size_t)b * kNB * kNB;
+        if (bwd) pre_diag_kernel<true><<<1, 256, kPreDiagSmem, st>>>(n, c, r0, sz, Wb, R, X);
+        else pre_diag_kernel<false><<<1, 256, kPreDiagSmem, st>>>(n, c, r0, sz, Wb, R, X);
+        RC_TRY(check_launch());
+        const int64_t rb = bwd ? 0 : r0 + sz, re = bwd ? r0 : n;
+        if (re > rb) {
+            const unsigned g = ceil_div(re - rb, 64);
+            if (bwd) pre_update_kernel<true><<<g, 256, kPreUpdSmem, st>>>(n, c, r0, sz, rb, re, W, ldw, X, R);
+            else pre_update_kernel<false><<<g, 256, kPreUpdSmem, st>>>(n, c, r0, sz, rb, re, W, ldw, X, R);
+            RC_TRY(check_launch());
+        }
+    }
+    return RC_SUCCESS;
+}
+
+int set_pre_smem() {
+    if (cudaFuncSetAttribute(pre_diag_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPreDiagSmem) ||
+        cudaFuncSetAttribute(pre_diag_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPreDiagSmem) ||
+        cudaFuncSetAttribute(pre_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPreUpdSmem) ||
+        cudaFuncSetAttribute(pre_update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPreUpdSmem))
+        return RC_ERR_CUDA;
+    return RC_SUCCESS;
+}
+
 dim3 vec_grid(int64_t n, int64_t c) {
     return dim3(ceil_div(n, 256) < 256u ? ceil_div(n, 256) : 256u, c < 65535 ? (unsigned)c : 65535u);
 }
@@ -165,6 +297,7 @@ int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* 
     add((size_t)n * sizeof(double));                    // column sums
     for (int i = 0; i < 4; ++i) add((size_t)n * nrhs * sizeof(double));  // R, Z, P, Q
     add((size_t)n * nrhs * sizeof(float));              // FP32 right-hand side of the preconditioner
+    add((size_t)n * nrhs * sizeof(float));              // FP32 intermediate of the preconditioner
     add((size_t)kNB * nrhs * sizeof(float));            // TRSM tile buffer
     add((size_t)8 * nrhs * sizeof(double));             // per-column scalars
     *bytes = b;
@@ -187,6 +320,7 @@ struct Mixed {
     double* colsum;
     double *R, *Z, *P, *Q;
     float* T32;
+    float* T32b;
     float* tmp;
     double* dev_scalars;  // 8 x nrhs
     View<const double> Av() const { return {A, 1, lda}; }
@@ -238,10 +372,13 @@ struct Mixed {
         const dim3 g = vec_grid(n, nrhs);
         to_f32_scaled_kernel<<<g, 256, 0, st>>>(n, nrhs, sc, Rin, ldr, T32);
         RC_TRY(check_launch());
-        const View<const float> L = {W, ldw, 1};
-        const View<float> Tv = colmajor(T32, n);
-        RC_TRY(trsm_preinv<float>(false, n, nrhs, L, Winv, Tv, tmp, st));
-        RC_TRY(trsm_preinv<float>(true, n, nrhs, L, Winv, Tv, tmp, st));
+        for (int64_t c0 = 0; c0 < nrhs; c0 += RHS) {  // column chunks of at most 64
+            const int c = (int)((nrhs - c0) < RHS ? nrhs - c0 : RHS);
+            float* R1 = T32 + c0 * n;
+            float* R2 = T32b + c0 * n;
+            RC_TRY(trsm_few(false, n, c, W, ldw, Winv, R1, R2, st));  // R2 = L^-1 R1
+            RC_TRY(trsm_few(true, n, c, W, ldw, Winv, R2, R1, st));   // R1 = L^-T R2
+        }
         from_f32_scaled_kernel<<<g, 256, 0, st>>>(n, nrhs, sc, T32, Zout, ldz);
         return check_launch();
     }
@@ -347,6 +484,7 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     M.P = buf.take<double>((size_t)n * nrhs);
     M.Q = buf.take<double>((size_t)n * nrhs);
     M.T32 = buf.take<float>((size_t)n * nrhs);
+    M.T32b = buf.take<float>((size_t)n * nrhs);
     M.tmp = buf.take<float>((size_t)kNB * nrhs);
     M.dev_scalars = buf.take<double>((size_t)8 * nrhs);
 
@@ -392,7 +530,9 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     std::vector<double> normB, normX, normR, rz, pq, alpha(nrhs), beta(nrhs);
     RC_TRY(M.col_reduce(B, ldb, nullptr, 0, 0, normB, M.dev_scalars));
 
-    // x0 = M^-1 b
+    // x0 = M^-1 b (the preconditioner kernels' shared-memory limits are raised here,
+    // outside the stream capture that later records the preconditioner as a graph)
+    RC_TRY(set_pre_smem());
     RC_TRY(M.precond(B, ldb, X, ldx));
     std::vector<char> done(nrhs, 0);
     int iters = 0, residuals = 0;
