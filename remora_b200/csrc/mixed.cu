@@ -137,45 +137,61 @@ __global__ void from_f32_scaled_kernel(int64_t n, int64_t c, const double* s, co
 
 // ---------------------------------------------------------------------------------------
 // Few-right-hand-side triangular solves with the FP32 factor (the CG preconditioner).
-// L is the row-major lower factor (ldw), Winv the row-major inverses of its kNB x kNB
-// diagonal blocks, right-hand sides column-major n x c (c <= 64, ld n). One block step
-// is two launches with every operand resident in shared memory (no k-loop barriers):
-//   diag:   X_b = M_b R_b          M_b = inv(L_bb) (forward) or inv(L_bb)^T (backward)
-//   update: forward  R[r0+sz:]  -= L[r0+sz:, r0:r0+sz] X_b
-//           backward R[:r0]     -= L[r0:r0+sz, :r0]^T   X_b
+// L is the row-major lower factor (ldw); Y holds the row-major inverses of its BS x BS
+// diagonal blocks (BS = 512, built once per solve from the 128-block inverses of the
+// factorisation); right-hand sides are column-major n x c (c <= 64, ld n). One block
+// step is two launches spread over many CTAs:
+//   diag:   X_b = M_b R_b      M_b = inv(L_bb) (forward) or inv(L_bb)^T (backward)
+//   update: forward  R[r0+sz:] -= L[r0+sz:, r0:r0+sz] X_b
+//           backward R[:r0]    -= L[r0:r0+sz, :r0]^T   X_b
+// with K consumed in 128-wide chunks staged in shared memory.
 constexpr int RHS = 64;
-constexpr int DP = kNB + 1;  // padded pitch of the inverse block in shared memory
+constexpr int BS = 512;     // diagonal block of the preconditioner solves
+constexpr int KC = 128;     // K chunk staged in shared memory
+constexpr int AP = 64 + 4;  // pitch of a staged 64-wide operand chunk
+constexpr int KCU = 64;     // K chunk of the update kernel (static shared memory <= 48 KB)
 
+// 16 rows of X_b per CTA: X_b[i, :] = sum_k M_b(i, k) R_b(k, :).
 template <bool BWD>
-__global__ void __launch_bounds__(256) pre_diag_kernel(int64_t n, int c, int64_t r0, int sz, const float* Winv_b,
+__global__ void __launch_bounds__(256) pre_diag_kernel(int64_t n, int c, int64_t r0, int sz, const float* Yb,
                                                        const float* R, float* X) {
-    extern __shared__ float sm[];
-    float* M = sm;                  // kNB x DP: M[i * DP + k] = M_b(i, k)
-    float* Rb = sm + kNB * DP;      // kNB x RHS: Rb[k * RHS + j]
+    __shared__ float Ms[KC][16 + 1];     // Ms[k][i]
+    __shared__ __align__(16) float Rs[KC][RHS];
     const int tid = threadIdx.x;
-    for (int e = tid; e < kNB * kNB; e += 256) {
-        const int a = e / kNB, b = e % kNB;  // Winv_b[a][b], coalesced
-        const float v = (a < sz && b < sz) ? Winv_b[e] : 0.f;
-        if (BWD) M[b * DP + a] = v; else M[a * DP + b] = v;
+    const int i0 = blockIdx.x * 16;
+    const int ti = tid / 16, tj = tid % 16;  // 16 x 16 threads: row ti, columns tj*4..+3
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int k0 = 0; k0 < sz; k0 += KC) {
+        for (int e = tid; e < 16 * KC; e += 256) {
+            float v = 0.f;
+            int ii, kk;
+            if (!BWD) {  // M(i, k) = Y(i, k): row i contiguous in k
+                ii = e / KC; kk = e % KC;
+                if (i0 + ii < sz && k0 + kk < sz) v = Yb[(int64_t)(i0 + ii) * BS + k0 + kk];
+            } else {     // M(i, k) = Y(k, i): row k contiguous in i
+                kk = e / 16; ii = e % 16;
+                if (i0 + ii < sz && k0 + kk < sz) v = Yb[(int64_t)(k0 + kk) * BS + i0 + ii];
+            }
+            Ms[kk][ii] = v;
+        }
+        for (int e = tid; e < KC * RHS; e += 256) {
+            const int kk = e % KC, j = e / KC;
+            Rs[kk][j] = (k0 + kk < sz && j < c) ? R[(r0 + k0 + kk) + (int64_t)j * n] : 0.f;
+        }
+        __syncthreads();
+        const int kmax = (sz - k0) < KC ? sz - k0 : KC;
+        for (int kk = 0; kk < kmax; ++kk) {
+            const float m = Ms[kk][ti];
+            const float4 x = *reinterpret_cast<const float4*>(&Rs[kk][4 * tj]);
+            acc[0] = fmaf(m, x.x, acc[0]); acc[1] = fmaf(m, x.y, acc[1]);
+            acc[2] = fmaf(m, x.z, acc[2]); acc[3] = fmaf(m, x.w, acc[3]);
+        }
+        __syncthreads();
     }
-    for (int e = tid; e < kNB * RHS; e += 256) {
-        const int k = e % kNB, j = e / kNB;  // column j, row k: coalesced along k
-        Rb[k * RHS + j] = (k < sz && j < c) ? R[(r0 + k) + (int64_t)j * n] : 0.f;
-    }
-    __syncthreads();
-    const int i = tid % kNB, j0 = (tid / kNB) * 32;
-    float acc[32];
+    if (i0 + ti < sz)
 #pragma unroll
-    for (int q = 0; q < 32; ++q) acc[q] = 0.f;
-    for (int k = 0; k < kNB; ++k) {
-        const float m = M[i * DP + k];
-#pragma unroll
-        for (int q = 0; q < 32; ++q) acc[q] = fmaf(m, Rb[k * RHS + j0 + q], acc[q]);
-    }
-    if (i < sz)
-#pragma unroll
-        for (int q = 0; q < 32; ++q)
-            if (j0 + q < c) X[(r0 + i) + (int64_t)(j0 + q) * n] = acc[q];
+        for (int v = 0; v < 4; ++v)
+            if (4 * tj + v < c) X[(r0 + i0 + ti) + (int64_t)(4 * tj + v) * n] = acc[v];
 }
 
 // Rows [i0, i0 + 64) of R -= A_tile (64 x sz) * X_b (sz x c), A_tile from the factor.
@@ -183,41 +199,43 @@ template <bool BWD>
 __global__ void __launch_bounds__(256) pre_update_kernel(int64_t n, int c, int64_t r0, int sz, int64_t row_begin,
                                                          int64_t row_end, const float* W, int64_t ldw,
                                                          const float* X, float* R) {
-    constexpr int AP = 64 + 4;  // pitch of As[k][i]
-    extern __shared__ float sm[];
-    float* As = sm;               // kNB x AP
-    float* Xs = sm + kNB * AP;    // kNB x RHS
+    __shared__ __align__(16) float As[KCU][AP];
+    __shared__ __align__(16) float Xs[KCU][RHS];
     const int tid = threadIdx.x;
     const int64_t i0 = row_begin + (int64_t)blockIdx.x * 64;
-    for (int e = tid; e < 64 * kNB; e += 256) {
-        int ii, k;
-        float v = 0.f;
-        if (!BWD) {  // A(i, k) = L(i, r0 + k): row i of L is contiguous in k
-            ii = e / kNB; k = e % kNB;
-            const int64_t gi = i0 + ii;
-            if (gi < row_end && k < sz) v = W[gi * ldw + r0 + k];
-        } else {     // A(i, k) = L(r0 + k, i): row r0 + k of L is contiguous in i
-            k = e / 64; ii = e % 64;
-            const int64_t gi = i0 + ii;
-            if (gi < row_end && k < sz) v = W[(r0 + k) * ldw + gi];
-        }
-        As[k * AP + ii] = v;
-    }
-    for (int e = tid; e < kNB * RHS; e += 256) {
-        const int k = e % kNB, j = e / kNB;
-        Xs[k * RHS + j] = (k < sz && j < c) ? X[(r0 + k) + (int64_t)j * n] : 0.f;
-    }
-    __syncthreads();
     const int tr = tid / 16, tc = tid % 16;
     float acc[4][4] = {};
-    for (int k = 0; k < sz; ++k) {
-        const float4 a = *reinterpret_cast<const float4*>(As + k * AP + 4 * tr);
-        const float4 x = *reinterpret_cast<const float4*>(Xs + k * RHS + 4 * tc);
-        const float av[4] = {a.x, a.y, a.z, a.w}, xv[4] = {x.x, x.y, x.z, x.w};
+    for (int k0 = 0; k0 < sz; k0 += KCU) {
+        for (int e = tid; e < 64 * KCU; e += 256) {
+            int ii, k;
+            float v = 0.f;
+            if (!BWD) {  // A(i, k) = L(i, r0 + k): row i of L contiguous in k
+                ii = e / KCU; k = e % KCU;
+                const int64_t gi = i0 + ii;
+                if (gi < row_end && k0 + k < sz) v = W[gi * ldw + r0 + k0 + k];
+            } else {     // A(i, k) = L(r0 + k, i): row r0 + k of L contiguous in i
+                k = e / 64; ii = e % 64;
+                const int64_t gi = i0 + ii;
+                if (gi < row_end && k0 + k < sz) v = W[(r0 + k0 + k) * ldw + gi];
+            }
+            As[k][ii] = v;
+        }
+        for (int e = tid; e < KCU * RHS; e += 256) {
+            const int k = e % KCU, j = e / KCU;
+            Xs[k][j] = (k0 + k < sz && j < c) ? X[(r0 + k0 + k) + (int64_t)j * n] : 0.f;
+        }
+        __syncthreads();
+        const int kmax = (sz - k0) < KCU ? sz - k0 : KCU;
+        for (int k = 0; k < kmax; ++k) {
+            const float4 a = *reinterpret_cast<const float4*>(&As[k][4 * tr]);
+            const float4 x = *reinterpret_cast<const float4*>(&Xs[k][4 * tc]);
+            const float av[4] = {a.x, a.y, a.z, a.w}, xv[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < 4; ++u)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], xv[v], acc[u][v]);
+                for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], xv[v], acc[u][v]);
+        }
+        __syncthreads();
     }
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
@@ -231,39 +249,61 @@ __global__ void __launch_bounds__(256) pre_update_kernel(int64_t n, int c, int64
     }
 }
 
-constexpr size_t kPreDiagSmem = (size_t)(kNB * DP + kNB * RHS) * sizeof(float);
-constexpr size_t kPreUpdSmem = (size_t)(kNB * (64 + 4) + kNB * RHS) * sizeof(float);
-
 // Solve L X = R (bwd = false) or L^T X = R (bwd = true) for c <= 64 columns; R is
 // consumed (updated in place), X receives the solution.
-int trsm_few(bool bwd, int64_t n, int c, const float* W, int64_t ldw, const float* Winv, float* R, float* X,
+int trsm_few(bool bwd, int64_t n, int c, const float* W, int64_t ldw, const float* Y, float* R, float* X,
              cudaStream_t st) {
-    const int64_t nblk = (n + kNB - 1) / kNB;
+    const int64_t nblk = (n + BS - 1) / BS;
     for (int64_t step = 0; step < nblk; ++step) {
         const int64_t b = bwd ? nblk - 1 - step : step;
-        const int64_t r0 = b * kNB;
-        const int sz = (int)((n - r0) < kNB ? n - r0 : kNB);
-        const float* Wb = Winv + (size_t)b * kNB * kNB;
-        if (bwd) pre_diag_kernel<true><<<1, 256, kPreDiagSmem, st>>>(n, c, r0, sz, Wb, R, X);
-        else pre_diag_kernel<false><<<1, 256, kPreDiagSmem, st>>>(n, c, r0, sz, Wb, R, X);
+        const int64_t r0 = b * BS;
+        const int sz = (int)((n - r0) < BS ? n - r0 : BS);
+        const float* Yb = Y + (size_t)b * BS * BS;
+        const unsigned gd = ceil_div(sz, 16);
+        if (bwd) pre_diag_kernel<true><<<gd, 256, 0, st>>>(n, c, r0, sz, Yb, R, X);
+        else pre_diag_kernel<false><<<gd, 256, 0, st>>>(n, c, r0, sz, Yb, R, X);
         RC_TRY(check_launch());
         const int64_t rb = bwd ? 0 : r0 + sz, re = bwd ? r0 : n;
         if (re > rb) {
             const unsigned g = ceil_div(re - rb, 64);
-            if (bwd) pre_update_kernel<true><<<g, 256, kPreUpdSmem, st>>>(n, c, r0, sz, rb, re, W, ldw, X, R);
-            else pre_update_kernel<false><<<g, 256, kPreUpdSmem, st>>>(n, c, r0, sz, rb, re, W, ldw, X, R);
+            if (bwd) pre_update_kernel<true><<<g, 256, 0, st>>>(n, c, r0, sz, rb, re, W, ldw, X, R);
+            else pre_update_kernel<false><<<g, 256, 0, st>>>(n, c, r0, sz, rb, re, W, ldw, X, R);
             RC_TRY(check_launch());
         }
     }
     return RC_SUCCESS;
 }
 
-int set_pre_smem() {
-    if (cudaFuncSetAttribute(pre_diag_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPreDiagSmem) ||
-        cudaFuncSetAttribute(pre_diag_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPreDiagSmem) ||
-        cudaFuncSetAttribute(pre_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPreUpdSmem) ||
-        cudaFuncSetAttribute(pre_update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPreUpdSmem))
-        return RC_ERR_CUDA;
+// Inverses of the BS x BS diagonal blocks of L (row-major, ld BS, zero above the
+// diagonal) from the 128-block inverses Winv: inv([A 0; C D]) = [inv(A) 0; -inv(D) C
+// inv(A) inv(D)], applied at 256 and then at 512. T is a BS x BS scratch block.
+int build_block_inverses(int64_t n, const float* W, int64_t ldw, const float* Winv, float* Y, float* T,
+                         cudaStream_t st) {
+    const int64_t nblk = (n + BS - 1) / BS;
+    if (cudaMemsetAsync(Y, 0, (size_t)nblk * BS * BS * sizeof(float), st) != cudaSuccess) return RC_ERR_CUDA;
+    const View<const float> L = {W, ldw, 1};
+    for (int64_t b = 0; b < nblk; ++b) {
+        const int64_t r0 = b * BS;
+        const int64_t sz = (n - r0) < BS ? n - r0 : BS;
+        const View<float> Xb = {Y + (size_t)b * BS * BS, BS, 1};
+        for (int64_t q = 0; q * kNB < sz; ++q) {
+            const int64_t qs = (sz - q * kNB) < kNB ? sz - q * kNB : kNB;
+            const float* src = Winv + (size_t)(r0 / kNB + q) * kNB * kNB;
+            RC_TRY(copy2d<float, float>(qs, qs, 1.f, View<const float>{src, kNB, 1}, Xb.sub(q * kNB, q * kNB), st));
+        }
+        for (int64_t h = kNB; h < BS; h *= 2) {        // half-size of the blocks being merged
+            for (int64_t p0 = 0; p0 + h < sz; p0 += 2 * h) {
+                const int64_t d = (sz - p0 - h) < h ? sz - p0 - h : h;  // rows of the lower half
+                const View<const float> Ainv = {Xb.p + p0 * BS + p0, BS, 1};
+                const View<const float> Dinv = {Xb.p + (p0 + h) * BS + (p0 + h), BS, 1};
+                const View<const float> C = L.sub(r0 + p0 + h, r0 + p0);
+                const View<float> Tv = {T, BS, 1};
+                RC_TRY(gemm<float>(d, h, h, 1.f, C, Ainv, 0.f, Tv, kFull, 0, st));
+                RC_TRY(gemm<float>(d, h, d, -1.f, Dinv, View<const float>{T, BS, 1}, 0.f,
+                                   Xb.sub(p0 + h, p0), kFull, 0, st));
+            }
+        }
+    }
     return RC_SUCCESS;
 }
 
@@ -299,6 +339,8 @@ int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* 
     add((size_t)n * nrhs * sizeof(float));              // FP32 right-hand side of the preconditioner
     add((size_t)n * nrhs * sizeof(float));              // FP32 intermediate of the preconditioner
     add((size_t)kNB * nrhs * sizeof(float));            // TRSM tile buffer
+    add((size_t)((n + 511) / 512) * 512 * 512 * sizeof(float));  // 512-block inverses
+    add((size_t)512 * 512 * sizeof(float));             // their scratch
     add((size_t)8 * nrhs * sizeof(double));             // per-column scalars
     *bytes = b;
     return RC_SUCCESS;
@@ -321,6 +363,8 @@ struct Mixed {
     double *R, *Z, *P, *Q;
     float* T32;
     float* T32b;
+    float* Y512;
+    float* Tinv;
     float* tmp;
     double* dev_scalars;  // 8 x nrhs
     View<const double> Av() const { return {A, 1, lda}; }
@@ -376,8 +420,8 @@ struct Mixed {
             const int c = (int)((nrhs - c0) < RHS ? nrhs - c0 : RHS);
             float* R1 = T32 + c0 * n;
             float* R2 = T32b + c0 * n;
-            RC_TRY(trsm_few(false, n, c, W, ldw, Winv, R1, R2, st));  // R2 = L^-1 R1
-            RC_TRY(trsm_few(true, n, c, W, ldw, Winv, R2, R1, st));   // R1 = L^-T R2
+            RC_TRY(trsm_few(false, n, c, W, ldw, Y512, R1, R2, st));  // R2 = L^-1 R1
+            RC_TRY(trsm_few(true, n, c, W, ldw, Y512, R2, R1, st));   // R1 = L^-T R2
         }
         from_f32_scaled_kernel<<<g, 256, 0, st>>>(n, nrhs, sc, T32, Zout, ldz);
         return check_launch();
@@ -486,6 +530,8 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     M.T32 = buf.take<float>((size_t)n * nrhs);
     M.T32b = buf.take<float>((size_t)n * nrhs);
     M.tmp = buf.take<float>((size_t)kNB * nrhs);
+    M.Y512 = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS);
+    M.Tinv = buf.take<float>((size_t)BS * BS);
     M.dev_scalars = buf.take<double>((size_t)8 * nrhs);
 
     cudaEvent_t e0, e1, e2;
@@ -530,9 +576,8 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     std::vector<double> normB, normX, normR, rz, pq, alpha(nrhs), beta(nrhs);
     RC_TRY(M.col_reduce(B, ldb, nullptr, 0, 0, normB, M.dev_scalars));
 
-    // x0 = M^-1 b (the preconditioner kernels' shared-memory limits are raised here,
-    // outside the stream capture that later records the preconditioner as a graph)
-    RC_TRY(set_pre_smem());
+    // x0 = M^-1 b, with the 512-block inverses built first
+    RC_TRY(build_block_inverses(n, M.W, M.ldw, M.Winv, M.Y512, M.Tinv, s));
     RC_TRY(M.precond(B, ldb, X, ldx));
     std::vector<char> done(nrhs, 0);
     int iters = 0, residuals = 0;
