@@ -123,152 +123,215 @@ __global__ void col_xpby_kernel(int64_t n, int64_t c, const double* b, const dou
     }
 }
 
-// T = fl32(s .* R) (row scaling) and back: Z = s .* T.
-__global__ void to_f32_scaled_kernel(int64_t n, int64_t c, const double* s, const double* R, int64_t ldr, float* T) {
-    for (int64_t j = blockIdx.y; j < c; j += gridDim.y)
-        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-            T[i + j * n] = (float)(s[i] * R[i + j * ldr]);
-}
-__global__ void from_f32_scaled_kernel(int64_t n, int64_t c, const double* s, const float* T, double* Z, int64_t ldz) {
-    for (int64_t j = blockIdx.y; j < c; j += gridDim.y)
-        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-            Z[i + j * ldz] = s[i] * (double)T[i + j * n];
-}
-
 // ---------------------------------------------------------------------------------------
 // Few-right-hand-side triangular solves with the FP32 factor (the CG preconditioner).
 // L is the row-major lower factor (ldw); Y holds the row-major inverses of its BS x BS
 // diagonal blocks (BS = 512, built once per solve from the 128-block inverses of the
-// factorisation); right-hand sides are column-major n x c (c <= 64, ld n). One block
-// step is two launches spread over many CTAs:
+// factorisation). The FP32 right-hand sides live in 64-column chunks, row-major inside a
+// chunk (element (i, j) of chunk q at q n 64 + i 64 + j, padding columns zero), so a K
+// slice of a chunk is one contiguous run. One block step is two launches of the same
+// register-blocked SIMT kernel:
 //   diag:   X_b = M_b R_b      M_b = inv(L_bb) (forward) or inv(L_bb)^T (backward)
 //   update: forward  R[r0+sz:] -= L[r0+sz:, r0:r0+sz] X_b
 //           backward R[:r0]    -= L[r0:r0+sz, :r0]^T   X_b
-// with K consumed in 128-wide chunks staged in shared memory.
 constexpr int RHS = 64;
-constexpr int BS = 512;     // diagonal block of the preconditioner solves
-constexpr int KC = 128;     // K chunk staged in shared memory
-constexpr int AP = 64 + 4;  // pitch of a staged 64-wide operand chunk
-constexpr int KCU = 64;     // K chunk of the update kernel (static shared memory <= 48 KB)
+constexpr int BS = 512;  // diagonal block of the preconditioner solves
+constexpr int UK = 32;   // K slice staged in shared memory
 
-// 16 rows of X_b per CTA: X_b[i, :] = sum_k M_b(i, k) R_b(k, :).
-template <bool BWD>
-__global__ void __launch_bounds__(256) pre_diag_kernel(int64_t n, int c, int64_t r0, int sz, const float* Yb,
-                                                       const float* R, float* X) {
-    __shared__ float Ms[KC][16 + 1];     // Ms[k][i]
-    __shared__ __align__(16) float Rs[KC][RHS];
-    const int tid = threadIdx.x;
-    const int i0 = blockIdx.x * 16;
-    const int ti = tid / 16, tj = tid % 16;  // 16 x 16 threads: row ti, columns tj*4..+3
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int k0 = 0; k0 < sz; k0 += KC) {
-        for (int e = tid; e < 16 * KC; e += 256) {
-            float v = 0.f;
-            int ii, kk;
-            if (!BWD) {  // M(i, k) = Y(i, k): row i contiguous in k
-                ii = e / KC; kk = e % KC;
-                if (i0 + ii < sz && k0 + kk < sz) v = Yb[(int64_t)(i0 + ii) * BS + k0 + kk];
-            } else {     // M(i, k) = Y(k, i): row k contiguous in i
-                kk = e / 16; ii = e % 16;
-                if (i0 + ii < sz && k0 + kk < sz) v = Yb[(int64_t)(k0 + kk) * BS + i0 + ii];
-            }
-            Ms[kk][ii] = v;
-        }
-        for (int e = tid; e < KC * RHS; e += 256) {
-            const int kk = e % KC, j = e / KC;
-            Rs[kk][j] = (k0 + kk < sz && j < c) ? R[(r0 + k0 + kk) + (int64_t)j * n] : 0.f;
-        }
-        __syncthreads();
-        const int kmax = (sz - k0) < KC ? sz - k0 : KC;
-        for (int kk = 0; kk < kmax; ++kk) {
-            const float m = Ms[kk][ti];
-            const float4 x = *reinterpret_cast<const float4*>(&Rs[kk][4 * tj]);
-            acc[0] = fmaf(m, x.x, acc[0]); acc[1] = fmaf(m, x.y, acc[1]);
-            acc[2] = fmaf(m, x.z, acc[2]); acc[3] = fmaf(m, x.w, acc[3]);
-        }
-        __syncthreads();
+// T = fl32(s .* R) in the chunked layout (R column-major, c columns), and back: Z = s .* T.
+// 32 x 32 tiles transposed through shared memory; grid (ceil(n/32), 2 ceil(c/64)).
+__global__ void to_f32_scaled_kernel(int64_t n, int64_t c, const double* s, const double* R, int64_t ldr, float* T) {
+    __shared__ float tile[32][33];
+    const int64_t i0 = (int64_t)blockIdx.x * 32, j0 = (int64_t)blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int64_t i = i0 + threadIdx.x, j = j0 + r;
+        tile[r][threadIdx.x] = (i < n && j < c) ? (float)(s[i] * R[i + j * ldr]) : 0.f;
     }
-    if (i0 + ti < sz)
-#pragma unroll
-        for (int v = 0; v < 4; ++v)
-            if (4 * tj + v < c) X[(r0 + i0 + ti) + (int64_t)(4 * tj + v) * n] = acc[v];
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int64_t i = i0 + r, j = j0 + threadIdx.x;
+        if (i < n) T[(j / RHS) * n * RHS + i * RHS + j % RHS] = tile[threadIdx.x][r];
+    }
 }
-
-// Rows [i0, i0 + 64) of R -= A_tile (64 x sz) * X_b (sz x c), A_tile from the factor.
-template <bool BWD>
-__global__ void __launch_bounds__(256) pre_update_kernel(int64_t n, int c, int64_t r0, int sz, int64_t row_begin,
-                                                         int64_t row_end, const float* W, int64_t ldw,
-                                                         const float* X, float* R) {
-    __shared__ __align__(16) float As[KCU][AP];
-    __shared__ __align__(16) float Xs[KCU][RHS];
-    const int tid = threadIdx.x;
-    const int64_t i0 = row_begin + (int64_t)blockIdx.x * 64;
-    const int tr = tid / 16, tc = tid % 16;
-    float acc[4][4] = {};
-    for (int k0 = 0; k0 < sz; k0 += KCU) {
-        for (int e = tid; e < 64 * KCU; e += 256) {
-            int ii, k;
-            float v = 0.f;
-            if (!BWD) {  // A(i, k) = L(i, r0 + k): row i of L contiguous in k
-                ii = e / KCU; k = e % KCU;
-                const int64_t gi = i0 + ii;
-                if (gi < row_end && k0 + k < sz) v = W[gi * ldw + r0 + k0 + k];
-            } else {     // A(i, k) = L(r0 + k, i): row r0 + k of L contiguous in i
-                k = e / 64; ii = e % 64;
-                const int64_t gi = i0 + ii;
-                if (gi < row_end && k0 + k < sz) v = W[(r0 + k0 + k) * ldw + gi];
-            }
-            As[k][ii] = v;
-        }
-        for (int e = tid; e < KCU * RHS; e += 256) {
-            const int k = e % KCU, j = e / KCU;
-            Xs[k][j] = (k0 + k < sz && j < c) ? X[(r0 + k0 + k) + (int64_t)j * n] : 0.f;
-        }
-        __syncthreads();
-        const int kmax = (sz - k0) < KCU ? sz - k0 : KCU;
-        for (int k = 0; k < kmax; ++k) {
-            const float4 a = *reinterpret_cast<const float4*>(&As[k][4 * tr]);
-            const float4 x = *reinterpret_cast<const float4*>(&Xs[k][4 * tc]);
-            const float av[4] = {a.x, a.y, a.z, a.w}, xv[4] = {x.x, x.y, x.z, x.w};
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], xv[v], acc[u][v]);
-        }
-        __syncthreads();
+__global__ void from_f32_scaled_kernel(int64_t n, int64_t c, const double* s, const float* T, double* Z, int64_t ldz) {
+    __shared__ float tile[32][33];
+    const int64_t i0 = (int64_t)blockIdx.x * 32, j0 = (int64_t)blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int64_t i = i0 + r, j = j0 + threadIdx.x;
+        tile[r][threadIdx.x] = i < n ? T[(j / RHS) * n * RHS + i * RHS + j % RHS] : 0.f;
     }
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        const int j = 4 * tc + v;
-        if (j >= c) continue;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int64_t gi = i0 + 4 * tr + u;
-            if (gi < row_end) R[gi + (int64_t)j * n] -= acc[u][v];
-        }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int64_t i = i0 + threadIdx.x, j = j0 + r;
+        if (i < n && j < c) Z[i + j * ldz] = s[i] * (double)tile[threadIdx.x][r];
     }
 }
 
-// Solve L X = R (bwd = false) or L^T X = R (bwd = true) for c <= 64 columns; R is
+// Rows [row_begin, row_end) of the 64-column chunk Out: Out (=, or -=) A X, with
+// A(i, k) = A[i lda + k] (TRANS = false) or A[k lda + i] (TRANS = true), k < K, and X the
+// K x 64 row-major slice. NT threads, 8 column groups of 8 and NT / 8 row groups of TM
+// rows: a CTA owns UM = NT TM / 8 rows. K is consumed in slices of UK staged in shared
+// memory through registers: the next slice is fetched while the current one is
+// multiplied. Requires lda % 4 == 0, A 16-byte aligned, and for TRANS row_begin % 4 == 0.
+template <bool TRANS, bool ASSIGN, int TM, int NT>
+__global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t row_end, int K, const float* A,
+                                                      int64_t lda, const float* X, float* Out) {
+    constexpr int UM = NT * TM / 8;
+    constexpr int UAP = UM + 4;
+    constexpr int NA = UM * UK / 4 / NT;   // float4 of A per thread and slice (= TM)
+    constexpr int NX = UK * RHS / 4 / NT;  // float4 of X per thread and slice
+    __shared__ __align__(16) float As[UK][UAP];
+    __shared__ __align__(16) float Xs[UK][RHS];
+    const int tid = threadIdx.x;
+    const int64_t i0 = row_begin + (int64_t)blockIdx.x * UM;
+    const int ty = tid / 8, tx = tid % 8;
+    float4 a_reg[NA], x_reg[NX];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < NA; ++q) {
+            const int e = tid + NT * q;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (!TRANS) {  // row ii, k = 4 kq .. 4 kq + 3
+                const int ii = e % UM, kq = e / UM;
+                const int64_t gi = i0 + ii;
+                const int k = k0 + 4 * kq;
+                if (gi < row_end) {
+                    const float* src = A + gi * lda + k;
+                    if (k + 3 < K) {
+                        v = *reinterpret_cast<const float4*>(src);
+                    } else {
+                        if (k < K) v.x = src[0];
+                        if (k + 1 < K) v.y = src[1];
+                        if (k + 2 < K) v.z = src[2];
+                    }
+                }
+            } else {       // row k, rows of the tile 4 g4 .. 4 g4 + 3
+                const int g4 = e % (UM / 4), k = k0 + e / (UM / 4);
+                const int64_t gi = i0 + 4 * g4;
+                if (k < K) {
+                    const float* src = A + (int64_t)k * lda + gi;
+                    if (gi + 3 < row_end) {
+                        v = *reinterpret_cast<const float4*>(src);
+                    } else {
+                        if (gi < row_end) v.x = src[0];
+                        if (gi + 1 < row_end) v.y = src[1];
+                        if (gi + 2 < row_end) v.z = src[2];
+                    }
+                }
+            }
+            a_reg[q] = v;
+        }
+#pragma unroll
+        for (int q = 0; q < NX; ++q) {
+            const int e = tid + NT * q;
+            const int k = k0 + e / (RHS / 4), c4 = e % (RHS / 4);
+            x_reg[q] = k < K ? *reinterpret_cast<const float4*>(X + (int64_t)k * RHS + 4 * c4)
+                             : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    };
+    auto stage = [&]() {
+#pragma unroll
+        for (int q = 0; q < NA; ++q) {
+            const int e = tid + NT * q;
+            if (!TRANS) {
+                const int ii = e % UM, kq = e / UM;
+                As[4 * kq + 0][ii] = a_reg[q].x;
+                As[4 * kq + 1][ii] = a_reg[q].y;
+                As[4 * kq + 2][ii] = a_reg[q].z;
+                As[4 * kq + 3][ii] = a_reg[q].w;
+            } else {
+                const int g4 = e % (UM / 4), k = e / (UM / 4);
+                *reinterpret_cast<float4*>(&As[k][4 * g4]) = a_reg[q];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NX; ++q) {
+            const int e = tid + NT * q;
+            *reinterpret_cast<float4*>(&Xs[e / (RHS / 4)][4 * (e % (RHS / 4))]) = x_reg[q];
+        }
+    };
+    float acc[TM][8];
+#pragma unroll
+    for (int u = 0; u < TM; ++u)
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[u][v] = 0.f;
+    fetch(0);
+    for (int k0 = 0; k0 < K; k0 += UK) {
+        stage();
+        __syncthreads();
+        if (k0 + UK < K) fetch(k0 + UK);
+#pragma unroll 4
+        for (int k = 0; k < UK; ++k) {  // slices past K are zero-filled
+            float av[TM];
+            if constexpr (TM % 4 == 0) {
+#pragma unroll
+                for (int u = 0; u < TM; u += 4) {
+                    const float4 t = *reinterpret_cast<const float4*>(&As[k][TM * ty + u]);
+                    av[u] = t.x; av[u + 1] = t.y; av[u + 2] = t.z; av[u + 3] = t.w;
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < TM; ++u) av[u] = As[k][TM * ty + u];
+            }
+            const float4 x0 = *reinterpret_cast<const float4*>(&Xs[k][8 * tx]);
+            const float4 x1 = *reinterpret_cast<const float4*>(&Xs[k][8 * tx + 4]);
+            const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+#pragma unroll
+            for (int u = 0; u < TM; ++u)
+#pragma unroll
+                for (int v = 0; v < 8; ++v) acc[u][v] = fmaf(av[u], xv[v], acc[u][v]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < TM; ++u) {
+        const int64_t gi = i0 + TM * ty + u;
+        if (gi >= row_end) continue;
+        float4* o = reinterpret_cast<float4*>(Out + gi * RHS + 8 * tx);
+        float4 lo = make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+        float4 hi = make_float4(acc[u][4], acc[u][5], acc[u][6], acc[u][7]);
+        if (!ASSIGN) {
+            const float4 p = o[0], r = o[1];
+            lo = make_float4(p.x - lo.x, p.y - lo.y, p.z - lo.z, p.w - lo.w);
+            hi = make_float4(r.x - hi.x, r.y - hi.y, r.z - hi.z, r.w - hi.w);
+        }
+        o[0] = lo;
+        o[1] = hi;
+    }
+}
+
+constexpr int kDiagTM = 2, kDiagNT = 64;  // 16-row tiles: 32 CTAs for a 512 block
+constexpr int kUpdTM = 8, kUpdNT = 64;    // 64-row tiles
+
+template <bool TRANS, bool ASSIGN, int TM, int NT>
+int launch_blk(int64_t rb, int64_t re, int K, const float* A, int64_t lda, const float* X, float* Out,
+               cudaStream_t st) {
+    constexpr int UM = NT * TM / 8;
+    blk_gemm_kernel<TRANS, ASSIGN, TM, NT><<<ceil_div(re - rb, UM), NT, 0, st>>>(rb, re, K, A, lda, X, Out);
+    return check_launch();
+}
+
+// Solve L X = R (bwd = false) or L^T X = R (bwd = true) for one 64-column chunk; R is
 // consumed (updated in place), X receives the solution.
-int trsm_few(bool bwd, int64_t n, int c, const float* W, int64_t ldw, const float* Y, float* R, float* X,
-             cudaStream_t st) {
+int trsm_few(bool bwd, int64_t n, const float* W, int64_t ldw, const float* Y, float* R, float* X, cudaStream_t st) {
+    if (ldw % 4 != 0 || reinterpret_cast<uintptr_t>(W) % 16 != 0 || reinterpret_cast<uintptr_t>(Y) % 16 != 0 ||
+        reinterpret_cast<uintptr_t>(R) % 16 != 0 || reinterpret_cast<uintptr_t>(X) % 16 != 0)
+        return RC_ERR_INVALID_ARGUMENT;
     const int64_t nblk = (n + BS - 1) / BS;
     for (int64_t step = 0; step < nblk; ++step) {
         const int64_t b = bwd ? nblk - 1 - step : step;
         const int64_t r0 = b * BS;
         const int sz = (int)((n - r0) < BS ? n - r0 : BS);
         const float* Yb = Y + (size_t)b * BS * BS;
-        const unsigned gd = ceil_div(sz, 16);
-        if (bwd) pre_diag_kernel<true><<<gd, 256, 0, st>>>(n, c, r0, sz, Yb, R, X);
-        else pre_diag_kernel<false><<<gd, 256, 0, st>>>(n, c, r0, sz, Yb, R, X);
-        RC_TRY(check_launch());
-        const int64_t rb = bwd ? 0 : r0 + sz, re = bwd ? r0 : n;
-        if (re > rb) {
-            const unsigned g = ceil_div(re - rb, 64);
-            if (bwd) pre_update_kernel<true><<<g, 256, 0, st>>>(n, c, r0, sz, rb, re, W, ldw, X, R);
-            else pre_update_kernel<false><<<g, 256, 0, st>>>(n, c, r0, sz, rb, re, W, ldw, X, R);
-            RC_TRY(check_launch());
+        const float* Rb = R + r0 * RHS;
+        float* Xb = X + r0 * RHS;
+        if (bwd) {
+            RC_TRY(launch_blk<true, true, kDiagTM, kDiagNT>(0, sz, sz, Yb, BS, Rb, Xb, st));
+            if (r0 > 0) RC_TRY(launch_blk<true, false, kUpdTM, kUpdNT>(0, r0, sz, W + r0 * ldw, ldw, Xb, R, st));
+        } else {
+            RC_TRY(launch_blk<false, true, kDiagTM, kDiagNT>(0, sz, sz, Yb, BS, Rb, Xb, st));
+            if (r0 + sz < n)
+                RC_TRY(launch_blk<false, false, kUpdTM, kUpdNT>(r0 + sz, n, sz, W + r0, ldw, Xb, R, st));
         }
     }
     return RC_SUCCESS;
@@ -336,8 +399,9 @@ int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* 
     add((size_t)n * sizeof(double));                    // s
     add((size_t)n * sizeof(double));                    // column sums
     for (int i = 0; i < 4; ++i) add((size_t)n * nrhs * sizeof(double));  // R, Z, P, Q
-    add((size_t)n * nrhs * sizeof(float));              // FP32 right-hand side of the preconditioner
-    add((size_t)n * nrhs * sizeof(float));              // FP32 intermediate of the preconditioner
+    const size_t chunked = (size_t)n * ((nrhs + RHS - 1) / RHS) * RHS;  // 64-column chunks
+    add(chunked * sizeof(float));                       // FP32 right-hand side of the preconditioner
+    add(chunked * sizeof(float));                       // FP32 intermediate of the preconditioner
     add((size_t)kNB * nrhs * sizeof(float));            // TRSM tile buffer
     add((size_t)((n + 511) / 512) * 512 * 512 * sizeof(float));  // 512-block inverses
     add((size_t)512 * 512 * sizeof(float));             // their scratch
@@ -413,17 +477,17 @@ struct Mixed {
 
     // Zout = M^-1 Rin = S L^-T L^-1 S Rin (FP64 in/out, FP32 triangular solves), on st.
     int precond_on(const double* Rin, int64_t ldr, double* Zout, int64_t ldz, cudaStream_t st) {
-        const dim3 g = vec_grid(n, nrhs);
-        to_f32_scaled_kernel<<<g, 256, 0, st>>>(n, nrhs, sc, Rin, ldr, T32);
+        const int64_t nch = (nrhs + RHS - 1) / RHS;  // 64-column chunks
+        const dim3 g(ceil_div(n, 32), (unsigned)(2 * nch)), tb(32, 8);
+        to_f32_scaled_kernel<<<g, tb, 0, st>>>(n, nrhs, sc, Rin, ldr, T32);
         RC_TRY(check_launch());
-        for (int64_t c0 = 0; c0 < nrhs; c0 += RHS) {  // column chunks of at most 64
-            const int c = (int)((nrhs - c0) < RHS ? nrhs - c0 : RHS);
-            float* R1 = T32 + c0 * n;
-            float* R2 = T32b + c0 * n;
-            RC_TRY(trsm_few(false, n, c, W, ldw, Y512, R1, R2, st));  // R2 = L^-1 R1
-            RC_TRY(trsm_few(true, n, c, W, ldw, Y512, R2, R1, st));   // R1 = L^-T R2
+        for (int64_t q = 0; q < nch; ++q) {
+            float* R1 = T32 + q * n * RHS;
+            float* R2 = T32b + q * n * RHS;
+            RC_TRY(trsm_few(false, n, W, ldw, Y512, R1, R2, st));  // R2 = L^-1 R1
+            RC_TRY(trsm_few(true, n, W, ldw, Y512, R2, R1, st));   // R1 = L^-T R2
         }
-        from_f32_scaled_kernel<<<g, 256, 0, st>>>(n, nrhs, sc, T32, Zout, ldz);
+        from_f32_scaled_kernel<<<g, tb, 0, st>>>(n, nrhs, sc, T32, Zout, ldz);
         return check_launch();
     }
     int precond(const double* Rin, int64_t ldr, double* Zout, int64_t ldz) {
@@ -527,8 +591,8 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     M.Z = buf.take<double>((size_t)n * nrhs);
     M.P = buf.take<double>((size_t)n * nrhs);
     M.Q = buf.take<double>((size_t)n * nrhs);
-    M.T32 = buf.take<float>((size_t)n * nrhs);
-    M.T32b = buf.take<float>((size_t)n * nrhs);
+    M.T32 = buf.take<float>((size_t)n * ((nrhs + RHS - 1) / RHS) * RHS);
+    M.T32b = buf.take<float>((size_t)n * ((nrhs + RHS - 1) / RHS) * RHS);
     M.tmp = buf.take<float>((size_t)kNB * nrhs);
     M.Y512 = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS);
     M.Tinv = buf.take<float>((size_t)BS * BS);
