@@ -19,7 +19,10 @@
 //         ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
 //     of the TRUE residual is at most tol (CG-based iterative refinement for SPD systems:
 //     Higham & Pranesh 2021; GMRES-IR: Carson & Higham 2017/2018).
+#include <cooperative_groups.h>
+
 #include <cmath>
+#include <cstdint>
 #include <vector>
 
 #include "assign.cuh"
@@ -27,6 +30,8 @@
 #include "gemm.cuh"
 #include "mixed.cuh"
 #include "tc_gemm.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace rc {
 namespace {
@@ -125,18 +130,21 @@ __global__ void col_xpby_kernel(int64_t n, int64_t c, const double* b, const dou
 
 // ---------------------------------------------------------------------------------------
 // Few-right-hand-side triangular solves with the FP32 factor (the CG preconditioner).
-// L is the row-major lower factor (ldw); Y holds the row-major inverses of its BS x BS
-// diagonal blocks (BS = 512, built once per solve from the 128-block inverses of the
-// factorisation). The FP32 right-hand sides live in 64-column chunks, row-major inside a
-// chunk (element (i, j) of chunk q at q n 64 + i 64 + j, padding columns zero), so a K
-// slice of a chunk is one contiguous run. One block step is two launches of the same
-// register-blocked SIMT kernel:
+// After the factorisation the lower triangle of W holds L and the strict upper triangle
+// is overwritten with L^T (W(i, j) = L(j, i) for j > i), so that both solve directions read
+// a contiguous ROW panel of W. Y holds the row-major inverses of the BS x BS diagonal
+// blocks (BS = 1024, built once per solve from the 128-block inverses of the
+// factorisation); block b occupies rows [b BS, (b + 1) BS) of the n x BS array Y. The
+// FP32 right-hand sides live in 64-column chunks, row-major inside a chunk (element
+// (i, j) of chunk q at q n 64 + i 64 + j, padding columns zero), so a K slice of a chunk
+// is one contiguous run. One block step is two launches of the same register-blocked
+// SIMT kernel:
 //   diag:   X_b = M_b R_b      M_b = inv(L_bb) (forward) or inv(L_bb)^T (backward)
-//   update: forward  R[r0+sz:] -= L[r0+sz:, r0:r0+sz] X_b
-//           backward R[:r0]    -= L[r0:r0+sz, :r0]^T   X_b
+//   update: forward  R[r0+sz:] -= L[r0+sz:, r0:r0+sz] X_b   (L^T rows of the upper part)
+//           backward R[:r0]    -= L[r0:r0+sz, :r0]^T   X_b   (L rows of the lower part)
 constexpr int RHS = 64;
-constexpr int BS = 512;  // diagonal block of the preconditioner solves
-constexpr int UK = 32;   // K slice staged in shared memory
+constexpr int BS = 1024;  // diagonal block of the preconditioner solves
+constexpr int UK = 32;    // K slice staged in shared memory
 
 // T = fl32(s .* R) in the chunked layout (R column-major, c columns), and back: Z = s .* T.
 // 32 x 32 tiles transposed through shared memory; grid (ceil(n/32), 2 ceil(c/64)).
@@ -167,12 +175,33 @@ __global__ void from_f32_scaled_kernel(int64_t n, int64_t c, const double* s, co
     }
 }
 
+// W(i, j) = W(j, i) for j > i: the strict upper triangle receives L^T. 32 x 32 tiles: the
+// CTA of upper tile (bi, bj), bj >= bi, reads lower tile (bj, bi) and writes it transposed.
+__global__ void mirror_lower_kernel(int64_t n, float* W, int64_t ldw) {
+    __shared__ float tile[32][33];
+    const int64_t bi = blockIdx.y, bj = blockIdx.x;
+    if (bj < bi) return;
+    for (int r = threadIdx.y; r < 32; r += 8) {  // lower tile rows bj*32 + r, columns bi*32 + tx
+        const int64_t i = bj * 32 + r, j = bi * 32 + threadIdx.x;
+        if (i < n && j <= i) tile[r][threadIdx.x] = W[i * ldw + j];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {  // upper tile rows bi*32 + r, columns bj*32 + tx
+        const int64_t i = bi * 32 + r, j = bj * 32 + threadIdx.x;
+        if (j < n && j > i) W[i * ldw + j] = tile[threadIdx.x][r];
+    }
+}
+
 // Rows [row_begin, row_end) of the 64-column chunk Out: Out (=, or -=) A X, with
 // A(i, k) = A[i lda + k] (TRANS = false) or A[k lda + i] (TRANS = true), k < K, and X the
-// K x 64 row-major slice. NT threads, 8 column groups of 8 and NT / 8 row groups of TM
-// rows: a CTA owns UM = NT TM / 8 rows. K is consumed in slices of UK staged in shared
-// memory through registers: the next slice is fetched while the current one is
-// multiplied. Requires lda % 4 == 0, A 16-byte aligned, and for TRANS row_begin % 4 == 0.
+// K x 64 row-major slice. NT threads in 8 column groups (columns 4 tx + {0..3} and
+// 32 + 4 tx + {0..3}) and NT / 8 row groups of TM rows: a CTA owns UM = NT TM / 8 rows.
+// K is split over the gridDim.y CTAs of a thread-block cluster (1, parts, 1); each takes
+// a contiguous run of UK-slices, staged in shared memory through registers (the next
+// slice is fetched while the current one is multiplied). The partial products are then
+// summed across the cluster through distributed shared memory in rank order (a
+// deterministic result), each CTA finishing UM / parts rows. Requires lda % 4 == 0, A,
+// X, Out 16-byte aligned, and for TRANS row_begin % 4 == 0.
 template <bool TRANS, bool ASSIGN, int TM, int NT>
 __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t row_end, int K, const float* A,
                                                       int64_t lda, const float* X, float* Out) {
@@ -180,11 +209,17 @@ __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t
     constexpr int UAP = UM + 4;
     constexpr int NA = UM * UK / 4 / NT;   // float4 of A per thread and slice (= TM)
     constexpr int NX = UK * RHS / 4 / NT;  // float4 of X per thread and slice
-    __shared__ __align__(16) float As[UK][UAP];
-    __shared__ __align__(16) float Xs[UK][RHS];
+    static_assert(UK * UAP + UK * RHS >= UM * RHS, "the reduction reuses the staging buffers");
+    __shared__ __align__(16) float sm[UK * UAP + UK * RHS];
+    float* As = sm;               // As[k * UAP + i]
+    float* Xs = sm + UK * UAP;    // Xs[k * RHS + j]
     const int tid = threadIdx.x;
     const int64_t i0 = row_begin + (int64_t)blockIdx.x * UM;
     const int ty = tid / 8, tx = tid % 8;
+    const int parts = gridDim.y, part = blockIdx.y;
+    const int kper = ((K + UK - 1) / UK + parts - 1) / parts * UK;  // whole slices per rank
+    const int kb = part * kper < K ? part * kper : K;
+    const int ke = kb + kper < K ? kb + kper : K;
     float4 a_reg[NA], x_reg[NX];
     auto fetch = [&](int k0) {
 #pragma unroll
@@ -197,18 +232,18 @@ __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t
                 const int k = k0 + 4 * kq;
                 if (gi < row_end) {
                     const float* src = A + gi * lda + k;
-                    if (k + 3 < K) {
+                    if (k + 3 < ke) {
                         v = *reinterpret_cast<const float4*>(src);
                     } else {
-                        if (k < K) v.x = src[0];
-                        if (k + 1 < K) v.y = src[1];
-                        if (k + 2 < K) v.z = src[2];
+                        if (k < ke) v.x = src[0];
+                        if (k + 1 < ke) v.y = src[1];
+                        if (k + 2 < ke) v.z = src[2];
                     }
                 }
             } else {       // row k, rows of the tile 4 g4 .. 4 g4 + 3
                 const int g4 = e % (UM / 4), k = k0 + e / (UM / 4);
                 const int64_t gi = i0 + 4 * g4;
-                if (k < K) {
+                if (k < ke) {
                     const float* src = A + (int64_t)k * lda + gi;
                     if (gi + 3 < row_end) {
                         v = *reinterpret_cast<const float4*>(src);
@@ -225,8 +260,8 @@ __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t
         for (int q = 0; q < NX; ++q) {
             const int e = tid + NT * q;
             const int k = k0 + e / (RHS / 4), c4 = e % (RHS / 4);
-            x_reg[q] = k < K ? *reinterpret_cast<const float4*>(X + (int64_t)k * RHS + 4 * c4)
-                             : make_float4(0.f, 0.f, 0.f, 0.f);
+            x_reg[q] = k < ke ? *reinterpret_cast<const float4*>(X + (int64_t)k * RHS + 4 * c4)
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
         }
     };
     auto stage = [&]() {
@@ -235,19 +270,19 @@ __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t
             const int e = tid + NT * q;
             if (!TRANS) {
                 const int ii = e % UM, kq = e / UM;
-                As[4 * kq + 0][ii] = a_reg[q].x;
-                As[4 * kq + 1][ii] = a_reg[q].y;
-                As[4 * kq + 2][ii] = a_reg[q].z;
-                As[4 * kq + 3][ii] = a_reg[q].w;
+                As[(4 * kq + 0) * UAP + ii] = a_reg[q].x;
+                As[(4 * kq + 1) * UAP + ii] = a_reg[q].y;
+                As[(4 * kq + 2) * UAP + ii] = a_reg[q].z;
+                As[(4 * kq + 3) * UAP + ii] = a_reg[q].w;
             } else {
                 const int g4 = e % (UM / 4), k = e / (UM / 4);
-                *reinterpret_cast<float4*>(&As[k][4 * g4]) = a_reg[q];
+                *reinterpret_cast<float4*>(&As[k * UAP + 4 * g4]) = a_reg[q];
             }
         }
 #pragma unroll
         for (int q = 0; q < NX; ++q) {
             const int e = tid + NT * q;
-            *reinterpret_cast<float4*>(&Xs[e / (RHS / 4)][4 * (e % (RHS / 4))]) = x_reg[q];
+            *reinterpret_cast<float4*>(&Xs[(e / (RHS / 4)) * RHS + 4 * (e % (RHS / 4))]) = x_reg[q];
         }
     };
     float acc[TM][8];
@@ -255,26 +290,26 @@ __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t
     for (int u = 0; u < TM; ++u)
 #pragma unroll
         for (int v = 0; v < 8; ++v) acc[u][v] = 0.f;
-    fetch(0);
-    for (int k0 = 0; k0 < K; k0 += UK) {
+    if (kb < ke) fetch(kb);
+    for (int k0 = kb; k0 < ke; k0 += UK) {
         stage();
         __syncthreads();
-        if (k0 + UK < K) fetch(k0 + UK);
+        if (k0 + UK < ke) fetch(k0 + UK);
 #pragma unroll 4
-        for (int k = 0; k < UK; ++k) {  // slices past K are zero-filled
+        for (int k = 0; k < UK; ++k) {  // slices past ke are zero-filled
             float av[TM];
             if constexpr (TM % 4 == 0) {
 #pragma unroll
                 for (int u = 0; u < TM; u += 4) {
-                    const float4 t = *reinterpret_cast<const float4*>(&As[k][TM * ty + u]);
+                    const float4 t = *reinterpret_cast<const float4*>(&As[k * UAP + TM * ty + u]);
                     av[u] = t.x; av[u + 1] = t.y; av[u + 2] = t.z; av[u + 3] = t.w;
                 }
             } else {
 #pragma unroll
-                for (int u = 0; u < TM; ++u) av[u] = As[k][TM * ty + u];
+                for (int u = 0; u < TM; ++u) av[u] = As[k * UAP + TM * ty + u];
             }
-            const float4 x0 = *reinterpret_cast<const float4*>(&Xs[k][8 * tx]);
-            const float4 x1 = *reinterpret_cast<const float4*>(&Xs[k][8 * tx + 4]);
+            const float4 x0 = *reinterpret_cast<const float4*>(&Xs[k * RHS + 4 * tx]);
+            const float4 x1 = *reinterpret_cast<const float4*>(&Xs[k * RHS + 32 + 4 * tx]);
             const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
 #pragma unroll
             for (int u = 0; u < TM; ++u)
@@ -283,36 +318,86 @@ __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t
         }
         __syncthreads();
     }
+    auto emit = [&](int64_t gi, int col, float4 v) {  // Out[gi, col..col+3] (=, -=) v
+        float4* o = reinterpret_cast<float4*>(Out + gi * RHS + col);
+        if (!ASSIGN) {
+            const float4 p = *o;
+            v = make_float4(p.x - v.x, p.y - v.y, p.z - v.z, p.w - v.w);
+        }
+        *o = v;
+    };
+    if (parts == 1) {
+#pragma unroll
+        for (int u = 0; u < TM; ++u) {
+            const int64_t gi = i0 + TM * ty + u;
+            if (gi >= row_end) continue;
+            emit(gi, 4 * tx, make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]));
+            emit(gi, 32 + 4 * tx, make_float4(acc[u][4], acc[u][5], acc[u][6], acc[u][7]));
+        }
+        return;
+    }
+    // Cluster reduction: partial tile (UM x 64, row-major) in this CTA's shared memory,
+    // then rank p sums rows [p UM / parts, (p + 1) UM / parts) over ranks 0..parts-1.
 #pragma unroll
     for (int u = 0; u < TM; ++u) {
-        const int64_t gi = i0 + TM * ty + u;
-        if (gi >= row_end) continue;
-        float4* o = reinterpret_cast<float4*>(Out + gi * RHS + 8 * tx);
-        float4 lo = make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
-        float4 hi = make_float4(acc[u][4], acc[u][5], acc[u][6], acc[u][7]);
-        if (!ASSIGN) {
-            const float4 p = o[0], r = o[1];
-            lo = make_float4(p.x - lo.x, p.y - lo.y, p.z - lo.z, p.w - lo.w);
-            hi = make_float4(r.x - hi.x, r.y - hi.y, r.z - hi.z, r.w - hi.w);
-        }
-        o[0] = lo;
-        o[1] = hi;
+        float* r = sm + (TM * ty + u) * RHS;
+        *reinterpret_cast<float4*>(r + 4 * tx) = make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+        *reinterpret_cast<float4*>(r + 32 + 4 * tx) = make_float4(acc[u][4], acc[u][5], acc[u][6], acc[u][7]);
     }
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    const int rows_per = UM / parts;
+    for (int e = tid; e < rows_per * (RHS / 4); e += NT) {
+        const int row = part * rows_per + e / (RHS / 4), col = 4 * (e % (RHS / 4));
+        float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int q = 0; q < parts; ++q) {
+            const float4 t = *reinterpret_cast<const float4*>(cluster.map_shared_rank(sm, q) + row * RHS + col);
+            sum.x += t.x; sum.y += t.y; sum.z += t.z; sum.w += t.w;
+        }
+        if (i0 + row < row_end) emit(i0 + row, col, sum);
+    }
+    cluster.sync();  // the other ranks may still read this CTA's partial tile
 }
 
-constexpr int kDiagTM = 2, kDiagNT = 64;  // 16-row tiles: 32 CTAs for a 512 block
-constexpr int kUpdTM = 8, kUpdNT = 64;    // 64-row tiles
+constexpr int kDiagTM = 2, kDiagNT = 64;  // 16-row tiles for the diagonal steps
+constexpr int kUpdTM = 8, kUpdNT = 64;    // 64-row tiles for the updates
 
+// Split K over a cluster of up to 8 CTAs so that the launch fills about one wave of
+// resident CTAs (slots = SMs x CTAs per SM) with at least two UK-slices per CTA.
 template <bool TRANS, bool ASSIGN, int TM, int NT>
 int launch_blk(int64_t rb, int64_t re, int K, const float* A, int64_t lda, const float* X, float* Out,
                cudaStream_t st) {
     constexpr int UM = NT * TM / 8;
-    blk_gemm_kernel<TRANS, ASSIGN, TM, NT><<<ceil_div(re - rb, UM), NT, 0, st>>>(rb, re, K, A, lda, X, Out);
+    static int slots = 0;
+    if (slots == 0) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, blk_gemm_kernel<TRANS, ASSIGN, TM, NT>, NT, 0) !=
+            cudaSuccess)
+            return RC_ERR_CUDA;
+        slots = (per_sm > 0 ? per_sm : 1) * sm_count();
+    }
+    const int64_t tiles = (re - rb + UM - 1) / UM;
+    int parts = 1;
+    while (parts < 8 && tiles * parts * 2 <= slots && K >= parts * 2 * 2 * UK) parts *= 2;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)tiles, (unsigned)parts, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = parts;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, blk_gemm_kernel<TRANS, ASSIGN, TM, NT>, rb, re, K, A, lda, X, Out) != cudaSuccess)
+        return RC_ERR_CUDA;
     return check_launch();
 }
 
 // Solve L X = R (bwd = false) or L^T X = R (bwd = true) for one 64-column chunk; R is
-// consumed (updated in place), X receives the solution.
+// consumed (updated in place), X receives the solution. W holds L below and L^T above
+// the diagonal.
 int trsm_few(bool bwd, int64_t n, const float* W, int64_t ldw, const float* Y, float* R, float* X, cudaStream_t st) {
     if (ldw % 4 != 0 || reinterpret_cast<uintptr_t>(W) % 16 != 0 || reinterpret_cast<uintptr_t>(Y) % 16 != 0 ||
         reinterpret_cast<uintptr_t>(R) % 16 != 0 || reinterpret_cast<uintptr_t>(X) % 16 != 0)
@@ -322,50 +407,115 @@ int trsm_few(bool bwd, int64_t n, const float* W, int64_t ldw, const float* Y, f
         const int64_t b = bwd ? nblk - 1 - step : step;
         const int64_t r0 = b * BS;
         const int sz = (int)((n - r0) < BS ? n - r0 : BS);
-        const float* Yb = Y + (size_t)b * BS * BS;
+        const float* Yb = Y + r0 * BS;
         const float* Rb = R + r0 * RHS;
         float* Xb = X + r0 * RHS;
+        const float* Wp = W + r0 * ldw;  // row panel [r0, r0 + sz)
         if (bwd) {
             RC_TRY(launch_blk<true, true, kDiagTM, kDiagNT>(0, sz, sz, Yb, BS, Rb, Xb, st));
-            if (r0 > 0) RC_TRY(launch_blk<true, false, kUpdTM, kUpdNT>(0, r0, sz, W + r0 * ldw, ldw, Xb, R, st));
+            if (r0 > 0) RC_TRY(launch_blk<true, false, kUpdTM, kUpdNT>(0, r0, sz, Wp, ldw, Xb, R, st));
         } else {
             RC_TRY(launch_blk<false, true, kDiagTM, kDiagNT>(0, sz, sz, Yb, BS, Rb, Xb, st));
-            if (r0 + sz < n)
-                RC_TRY(launch_blk<false, false, kUpdTM, kUpdNT>(r0 + sz, n, sz, W + r0, ldw, Xb, R, st));
+            if (r0 + sz < n) RC_TRY(launch_blk<true, false, kUpdTM, kUpdNT>(r0 + sz, n, sz, Wp, ldw, Xb, R, st));
         }
     }
     return RC_SUCCESS;
 }
 
-// Inverses of the BS x BS diagonal blocks of L (row-major, ld BS, zero above the
-// diagonal) from the 128-block inverses Winv: inv([A 0; C D]) = [inv(A) 0; -inv(D) C
-// inv(A) inv(D)], applied at 256 and then at 512. T is a BS x BS scratch block.
+// Batched C_z (=, alpha) A_z B_z for the block-inverse merges, one z per grid.z, 64 x 64
+// tiles of 256 threads (4 x 4 each). Operand z is at p + (z zr + i) ld + (z zc mod cm) + j:
+// the merges of one level sit at every 2h-aligned position of the n x n factor, and the
+// inverses of a BS block at its rows of the n x BS array Y.
+struct BatchView {
+    float* p;
+    int64_t ld, zr, zc, cm;
+    __device__ float* at(int64_t z, int64_t i, int64_t j) const { return p + (z * zr + i) * ld + (z * zc) % cm + j; }
+};
+// Merge level h: for each z with g = 2 h z, g + h < n, d = min(h, n - g - h):
+//   step 0: T_z = C_z Ainv_z   (d x h, k = h)
+//   step 1: X_z = -Dinv_z T_z  (d x h, k = d)
+__global__ void __launch_bounds__(256) merge_gemm_kernel(int64_t n, int64_t h, int step, BatchView A, BatchView B,
+                                                          BatchView C) {
+    constexpr int BM = 64, BN = 64, BK = 16;
+    __shared__ float sA[BK][BM + 1];
+    __shared__ float sB[BK][BN + 1];
+    const int64_t z = blockIdx.z, g = 2 * h * z;
+    if (g + h >= n) return;
+    const int64_t d = (n - g - h) < h ? n - g - h : h;
+    const int64_t m = d, nn = h, k = step == 0 ? h : d;
+    const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
+    if (m0 >= m) return;
+    const int tid = threadIdx.x, tm = tid / 16, tn = tid % 16;
+    float acc[4][4] = {};
+    for (int64_t k0 = 0; k0 < k; k0 += BK) {
+        for (int e = tid; e < BM * BK; e += 256) {
+            const int kk = e % BK, mm = e / BK;  // A rows are K-contiguous
+            sA[kk][mm] = (m0 + mm < m && k0 + kk < k) ? *A.at(z, m0 + mm, k0 + kk) : 0.f;
+            const int nb = e % BN, kb = e / BN;  // B rows are N-contiguous
+            sB[kb][nb] = (n0 + nb < nn && k0 + kb < k) ? *B.at(z, k0 + kb, n0 + nb) : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            float a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) a[r] = sA[kk][tm + 16 * r];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) b[c] = sB[kk][tn + 16 * c];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(a[r], b[c], acc[r][c]);
+        }
+        __syncthreads();
+    }
+    const float alpha = step == 0 ? 1.f : -1.f;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int64_t i = m0 + tm + 16 * r, j = n0 + tn + 16 * c;
+            if (i < m && j < nn) *C.at(z, i, j) = alpha * acc[r][c];
+        }
+}
+
+// Y rows [q kNB, q kNB + kNB), columns (q kNB mod BS) + [0, kNB) <- the 128-block inverse q.
+__global__ void place_inverses_kernel(int64_t n, const float* Winv, float* Y) {
+    const int64_t q = blockIdx.y;
+    const int64_t r0 = q * kNB, c0 = r0 % BS;
+    const int64_t qs = (n - r0) < kNB ? n - r0 : kNB;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < qs * qs; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e / qs, j = e % qs;
+        Y[(r0 + i) * BS + c0 + j] = Winv[q * kNB * kNB + i * kNB + j];
+    }
+}
+
+// Inverses of the BS x BS diagonal blocks of L (row-major rows of the n x BS array Y, zero
+// above the diagonal) from the 128-block inverses Winv: inv([A 0; C D]) = [inv(A) 0;
+// -inv(D) C inv(A)  inv(D)], applied level by level (h = 128, 256, ..., BS / 2) to every
+// block at once. T is an n x BS / 2 scratch array.
 int build_block_inverses(int64_t n, const float* W, int64_t ldw, const float* Winv, float* Y, float* T,
                          cudaStream_t st) {
     const int64_t nblk = (n + BS - 1) / BS;
     if (cudaMemsetAsync(Y, 0, (size_t)nblk * BS * BS * sizeof(float), st) != cudaSuccess) return RC_ERR_CUDA;
-    const View<const float> L = {W, ldw, 1};
-    for (int64_t b = 0; b < nblk; ++b) {
-        const int64_t r0 = b * BS;
-        const int64_t sz = (n - r0) < BS ? n - r0 : BS;
-        const View<float> Xb = {Y + (size_t)b * BS * BS, BS, 1};
-        for (int64_t q = 0; q * kNB < sz; ++q) {
-            const int64_t qs = (sz - q * kNB) < kNB ? sz - q * kNB : kNB;
-            const float* src = Winv + (size_t)(r0 / kNB + q) * kNB * kNB;
-            RC_TRY(copy2d<float, float>(qs, qs, 1.f, View<const float>{src, kNB, 1}, Xb.sub(q * kNB, q * kNB), st));
-        }
-        for (int64_t h = kNB; h < BS; h *= 2) {        // half-size of the blocks being merged
-            for (int64_t p0 = 0; p0 + h < sz; p0 += 2 * h) {
-                const int64_t d = (sz - p0 - h) < h ? sz - p0 - h : h;  // rows of the lower half
-                const View<const float> Ainv = {Xb.p + p0 * BS + p0, BS, 1};
-                const View<const float> Dinv = {Xb.p + (p0 + h) * BS + (p0 + h), BS, 1};
-                const View<const float> C = L.sub(r0 + p0 + h, r0 + p0);
-                const View<float> Tv = {T, BS, 1};
-                RC_TRY(gemm<float>(d, h, h, 1.f, C, Ainv, 0.f, Tv, kFull, 0, st));
-                RC_TRY(gemm<float>(d, h, d, -1.f, Dinv, View<const float>{T, BS, 1}, 0.f,
-                                   Xb.sub(p0 + h, p0), kFull, 0, st));
-            }
-        }
+    const int64_t nq = (n + kNB - 1) / kNB;
+    place_inverses_kernel<<<dim3(16, (unsigned)nq), 256, 0, st>>>(n, Winv, Y);
+    RC_TRY(check_launch());
+    const int64_t big = INT64_MAX / 4;
+    for (int64_t h = kNB; h < BS; h *= 2) {
+        const int64_t nz = (n + 2 * h - 1) / (2 * h);
+        const dim3 grid((unsigned)ceil_div(h, 64), (unsigned)ceil_div(h, 64), (unsigned)nz);
+        // T_z (d x h, ld h) = C_z Ainv_z: C_z = L(g + h.., g..), Ainv_z = Y rows g.., cols g mod BS
+        const BatchView C = {const_cast<float*>(W) + h * ldw, ldw, 2 * h, 2 * h, big};
+        const BatchView Ainv = {Y, BS, 2 * h, 2 * h, BS};
+        const BatchView Tv = {T, h, h, 0, big};
+        merge_gemm_kernel<<<grid, 256, 0, st>>>(n, h, 0, C, Ainv, Tv);
+        RC_TRY(check_launch());
+        // X_z = -Dinv_z T_z: Dinv_z = Y rows g + h.., cols (g + h) mod BS; X_z = Y rows g + h.., cols g mod BS
+        const BatchView Dinv = {Y + h * BS + h, BS, 2 * h, 2 * h, BS};
+        const BatchView Xz = {Y + h * BS, BS, 2 * h, 2 * h, BS};
+        merge_gemm_kernel<<<grid, 256, 0, st>>>(n, h, 1, Dinv, Tv, Xz);
+        RC_TRY(check_launch());
     }
     return RC_SUCCESS;
 }
@@ -403,8 +553,8 @@ int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* 
     add(chunked * sizeof(float));                       // FP32 right-hand side of the preconditioner
     add(chunked * sizeof(float));                       // FP32 intermediate of the preconditioner
     add((size_t)kNB * nrhs * sizeof(float));            // TRSM tile buffer
-    add((size_t)((n + 511) / 512) * 512 * 512 * sizeof(float));  // 512-block inverses
-    add((size_t)512 * 512 * sizeof(float));             // their scratch
+    add((size_t)((n + BS - 1) / BS) * BS * BS * sizeof(float));      // BS-block inverses
+    add((size_t)((n + BS - 1) / BS) * BS * BS / 2 * sizeof(float));  // their scratch
     add((size_t)8 * nrhs * sizeof(double));             // per-column scalars
     *bytes = b;
     return RC_SUCCESS;
@@ -427,7 +577,7 @@ struct Mixed {
     double *R, *Z, *P, *Q;
     float* T32;
     float* T32b;
-    float* Y512;
+    float* Y;  // BS-block inverses
     float* Tinv;
     float* tmp;
     double* dev_scalars;  // 8 x nrhs
@@ -484,8 +634,8 @@ struct Mixed {
         for (int64_t q = 0; q < nch; ++q) {
             float* R1 = T32 + q * n * RHS;
             float* R2 = T32b + q * n * RHS;
-            RC_TRY(trsm_few(false, n, W, ldw, Y512, R1, R2, st));  // R2 = L^-1 R1
-            RC_TRY(trsm_few(true, n, W, ldw, Y512, R2, R1, st));   // R1 = L^-T R2
+            RC_TRY(trsm_few(false, n, W, ldw, Y, R1, R2, st));  // R2 = L^-1 R1
+            RC_TRY(trsm_few(true, n, W, ldw, Y, R2, R1, st));   // R1 = L^-T R2
         }
         from_f32_scaled_kernel<<<g, tb, 0, st>>>(n, nrhs, sc, T32, Zout, ldz);
         return check_launch();
@@ -594,8 +744,8 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     M.T32 = buf.take<float>((size_t)n * ((nrhs + RHS - 1) / RHS) * RHS);
     M.T32b = buf.take<float>((size_t)n * ((nrhs + RHS - 1) / RHS) * RHS);
     M.tmp = buf.take<float>((size_t)kNB * nrhs);
-    M.Y512 = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS);
-    M.Tinv = buf.take<float>((size_t)BS * BS);
+    M.Y = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS);
+    M.Tinv = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS / 2);
     M.dev_scalars = buf.take<double>((size_t)8 * nrhs);
 
     cudaEvent_t e0, e1, e2;
@@ -640,8 +790,14 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     std::vector<double> normB, normX, normR, rz, pq, alpha(nrhs), beta(nrhs);
     RC_TRY(M.col_reduce(B, ldb, nullptr, 0, 0, normB, M.dev_scalars));
 
-    // x0 = M^-1 b, with the 512-block inverses built first
-    RC_TRY(build_block_inverses(n, M.W, M.ldw, M.Winv, M.Y512, M.Tinv, s));
+    // x0 = M^-1 b, after L^T is mirrored into W's upper triangle and the BS-block
+    // inverses are built
+    {
+        const unsigned nt = ceil_div(n, 32);
+        mirror_lower_kernel<<<dim3(nt, nt), dim3(32, 8), 0, s>>>(n, M.W, M.ldw);
+        RC_TRY(check_launch());
+    }
+    RC_TRY(build_block_inverses(n, M.W, M.ldw, M.Winv, M.Y, M.Tinv, s));
     RC_TRY(M.precond(B, ldb, X, ldx));
     std::vector<char> done(nrhs, 0);
     int iters = 0, residuals = 0;

@@ -91,3 +91,19 @@ def test_mixed_solve_not_spd_reports_pivot(cuda):
     A[200, 200] = -1.0
     X, info, status = ops.spd_solve_mixed(to_dev(A, False), to_dev(np.ones((n, 2)), False), "tf32")
     assert info["pivot"] == 201
+
+
+@pytest.mark.parametrize("n,nrhs", [(3100, 70), (4096, 64), (2048, 1)])
+def test_mixed_solve_block_steps_and_column_chunks(cuda, orc, n, nrhs):
+    """Several diagonal blocks of the preconditioner solves (a ragged last block at
+    n = 3100), right-hand sides spread over two 64-column chunks (nrhs = 70), exact
+    multiples of both, and a single column."""
+    A = spd_with_condition(n, 1e3, seed=n)
+    B = orc.rng(n).normal(n, nrhs)
+    X, info, status = ops.spd_solve_mixed(to_dev(A, False), to_dev(B, False), "tf32", max_iter=100)
+    assert status == 0 and info["converged"] == 1, info
+    Xh = to_host(X)
+    assert backward_error(A, Xh, B) <= 1e-15
+    ref = np.array(B, order="F")
+    assert orc.cholesky_solve(np.asfortranarray(A), ref) == 0
+    assert np.linalg.norm(Xh - ref) / np.linalg.norm(ref) <= 100 * 1e3 * U64
