@@ -86,123 +86,238 @@ __global__ void __launch_bounds__(NB) trtri_blocks(int64_t m, View<const T> L, b
     store_block<T>(S, W + (size_t)blockIdx.x * NB * NB);
 }
 
+// 1 / sqrt(d) for d > 0: a single-precision seed refined by two Newton-Raphson steps for
+// the reciprocal square root, r <- r (3 - d r^2) / 2 (quadratic convergence: ~2^-22 ->
+// ~2^-44 -> rounding level), which is much shorter than the double-precision library
+// call on the factorisation's critical path. Outside the float range: the library call.
+__device__ __forceinline__ double recip_sqrt(double d) {
+    if (!(d > 1e-30 && d < 1e30)) return rsqrt(d);
+    double r = (double)rsqrtf((float)d);
+    const double h = 0.5 * d;
+    r = r * fma(-h * r, r, 1.5);
+    r = r * fma(-h * r, r, 1.5);
+    return r;
+}
+
+// In-CTA blocked factorisation of one NB x NB diagonal block (FP64 in shared memory S,
+// row-major, odd stride SLD so that both row and column walks are bank-conflict free).
+// Besides L (lower triangle of S) it keeps rd[i] = 1 / L(i, i) and builds inv(L) in the
+// strict upper triangle: Inv(i, c), i > c, is stored at S[c * SLD + i].
+constexpr int DB = 32;  // diagonal sub-block
+constexpr size_t kDiagSmem = kBlockSmem + (NB + 64 * 65) * sizeof(double) + 16;  // S, rd, T, flag
+
+// S[i][c] -= sum_{m in [C0, C0 + DB)} L(i, m) L(c, m) for C0 + DB <= c <= i < NB. Thread
+// (ty, tx) of 16 x 16 owns rows ty + 16 r and columns tx + 16 q with r, q >= (C0 + DB) / 16.
+template <int KB>
+__device__ void trailing_update(double* S) {
+    constexpr int C0 = DB * KB, R0 = (C0 + DB) / 16, G = NB / 16 - R0;
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+    double acc[G][G];
+#pragma unroll
+    for (int r = 0; r < G; ++r)
+#pragma unroll
+        for (int q = 0; q < G; ++q) acc[r][q] = 0.0;
+#pragma unroll 4
+    for (int m = C0; m < C0 + DB; ++m) {
+        double lr[G], lc[G];
+#pragma unroll
+        for (int r = 0; r < G; ++r) lr[r] = S[(ty + 16 * (R0 + r)) * SLD + m];
+#pragma unroll
+        for (int q = 0; q < G; ++q) lc[q] = S[(tx + 16 * (R0 + q)) * SLD + m];
+#pragma unroll
+        for (int r = 0; r < G; ++r)
+#pragma unroll
+            for (int q = 0; q <= r; ++q) acc[r][q] = fma(lr[r], lc[q], acc[r][q]);
+    }
+#pragma unroll
+    for (int r = 0; r < G; ++r)
+#pragma unroll
+        for (int q = 0; q <= r; ++q) {
+            const int i = ty + 16 * (R0 + r), c = tx + 16 * (R0 + q);
+            if (c <= i) S[i * SLD + c] -= acc[r][q];
+        }
+}
+
+// One step of the recursive inverse, for blocks of H rows: with inv(A) (rows/columns
+// [J0, J0 + H)) and inv(D) ([I0, I0 + H), I0 = J0 + H) in place, the off-diagonal block of
+// inv([A 0; C D]) is X = -inv(D) (C inv(A)). Needs rd on the diagonal of S, so that
+// Inv(i, c) = S[c * SLD + i] for i >= c. NT threads (index t); thread (ty, tx) of
+// (NT / 16) x 16 computes rows ty + (NT / 16) r and columns tx + 16 q of the H x H
+// products; T is an H x H scratch (pitch 65). Phase 0: T = C inv(A); phase 1: X.
+template <int H, int NT>
+__device__ void inverse_merge(double* S, double* T, int J0, int t, int phase) {
+    constexpr int RY = NT / 16, NR = H / RY, NQ = H / 16;
+    const int I0 = J0 + H, ty = t / 16, tx = t % 16;
+    double acc[NR][NQ];
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) acc[r][q] = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < H; ++k) {
+        double lr[NR], lc[NQ];
+        if (phase == 0) {  // C(i, k) = L(I0 + i, J0 + k); inv(A)(k, c) = S[(J0 + c) SLD + J0 + k], k >= c
+#pragma unroll
+            for (int r = 0; r < NR; ++r) lr[r] = S[(I0 + ty + RY * r) * SLD + J0 + k];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const int c = tx + 16 * q;
+                const double v = S[(J0 + c) * SLD + J0 + k];
+                lc[q] = k >= c ? v : 0.0;
+            }
+        } else {           // inv(D)(i, k) = S[(I0 + k) SLD + I0 + i], k <= i; T(k, c)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const int i = ty + RY * r;
+                const double v = S[(I0 + k) * SLD + I0 + i];
+                lr[r] = k <= i ? v : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) lc[q] = T[k * 65 + tx + 16 * q];
+        }
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) acc[r][q] = fma(lr[r], lc[q], acc[r][q]);
+    }
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const int i = ty + RY * r, c = tx + 16 * q;
+            if (phase == 0) T[i * 65 + c] = acc[r][q];
+            else S[(J0 + c) * SLD + I0 + i] = -acc[r][q];  // X(i, c) stored transposed
+        }
+}
+
 // Factor the sz x sz lower diagonal block (A already offset to it) in FP64 and store
 // inv(L) into W (column-major, or row-major when w_row_major); g0 = global index of the
-// block for the pivot status. Register-blocked: thread (ty, tx) of the 16 x 16 CTA owns
-// the 8 x 8 elements (ty + 16 r, tx + 16 q) in registers; each column step broadcasts one
-// column through shared memory (two barriers per column), and the inverse is formed the
-// same way by right-looking forward substitution on the identity (one barrier per row,
-// double-buffered row broadcast).
+// block for the pivot status. Blocked in shared memory over 32-column sub-blocks k:
+//   1. warp 0 factors the 32 x 32 diagonal sub-block right-looking with each lane's row
+//      in registers (a column step: a shuffle of the pivot, one reciprocal square root,
+//      the column broadcast through shared memory and independent FMAs, no CTA barrier);
+//   2. warp 0 inverts that sub-block (each lane a column, in registers) while warps 1-3
+//      solve the rows below it (each thread a row, in registers), both right-looking
+//      substitutions reading L through shared-memory broadcasts;
+//   3. all threads apply the rank-32 update to the trailing triangle (register tiles).
+// inv(L) is then merged from the 32-block inverses: two 64-blocks at once, then the
+// 128-block (X = -inv(D) C inv(A) at each merge).
 template <class T>
 __global__ void __launch_bounds__(256, 1) potrf_diag(View<T> A, int sz, int64_t g0, T* W, int* info,
                                                      bool w_row_major) {
-    extern __shared__ double S[];  // NB x SLD: L after the factorisation
-    __shared__ double col[NB];
-    __shared__ double row2[2][NB];
-    __shared__ double piv;
+    extern __shared__ double S[];
+    double* rd = S + NB * SLD;
+    double* Tm = rd + NB;
+    int* fail = reinterpret_cast<int*>(Tm + 64 * 65);
     if (aborted(info)) return;
-    const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
-    double a[8][8];
-#pragma unroll
-    for (int r = 0; r < 8; ++r)
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int i = ty + 16 * r, c = tx + 16 * q;
-            a[r][q] = (i < sz && c < sz && c <= i) ? (double)A(i, c) : (i == c ? 1.0 : 0.0);
-        }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        for (int jj = 0; jj < 16; ++jj) {
-            const int j = 16 * q + jj;
-            if (j >= sz) break;
-            if (tx == jj && ty == jj) {
-                const double d = a[q][q];
-                piv = d > 0.0 ? sqrt(d) : -1.0;  // also catches NaN
-            }
-            __syncthreads();
-            const double sq = piv;
-            if (!(sq > 0.0)) {
-                if (tid == 0) record_first(info, (int)(g0 + j + 1));
-                return;
-            }
-            if (tx == jj) {
-                const double rsq = 1.0 / sq;  // one division per column, then products
-#pragma unroll
-                for (int r = 0; r < 8; ++r) {
-                    const int i = ty + 16 * r;
-                    double v = 0.0;
-                    if (i == j) v = sq;
-                    else if (i > j) v = a[r][q] * rsq;
-                    if (i >= j) a[r][q] = v;
-                    col[i] = v;
-                }
-            }
-            __syncthreads();
-            double lr[8], lc[8];
-#pragma unroll
-            for (int r = 0; r < 8; ++r) lr[r] = col[ty + 16 * r];
-#pragma unroll
-            for (int q2 = 0; q2 < 8; ++q2) lc[q2] = col[tx + 16 * q2];
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-#pragma unroll
-                for (int q2 = 0; q2 < 8; ++q2) {
-                    const int i = ty + 16 * r, c = tx + 16 * q2;
-                    if (c > j && i >= c) a[r][q2] = fma(-lr[r], lc[q2], a[r][q2]);
-                }
-        }
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool rowmaj = A.cs == 1;
+    for (int e = tid; e < NB * NB; e += 256) {
+        const int i = rowmaj ? e / NB : e % NB, c = rowmaj ? e % NB : e / NB;
+        S[i * SLD + c] = (i < sz && c < sz && c <= i) ? (double)A(i, c) : (i == c ? 1.0 : 0.0);
     }
-    // L back to global memory (lower part) and to shared memory for the inversion.
-#pragma unroll
-    for (int r = 0; r < 8; ++r)
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int i = ty + 16 * r, c = tx + 16 * q;
-            const double v = c <= i ? a[r][q] : 0.0;
-            S[i * SLD + c] = v;
-            if (i < sz && c <= i) A(i, c) = (T)v;
-        }
-    // Padding rows/columns beyond sz hold the identity, so the inverse is well defined.
-#pragma unroll
-    for (int r = 0; r < 8; ++r)
-#pragma unroll
-        for (int q = 0; q < 8; ++q) a[r][q] = (ty + 16 * r == tx + 16 * q) ? 1.0 : 0.0;
+    if (tid == 0) *fail = 0;
     __syncthreads();
+#pragma unroll 1
+    for (int kb = 0; kb < NB / DB; ++kb) {
+        const int c0 = DB * kb;
+        if (warp == 0) {  // 1. right-looking factor of the diagonal sub-block, row `lane` in registers
+            const int i = c0 + lane;
+            double a[DB];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        for (int kk = 0; kk < 16; ++kk) {
-            const int k = 16 * q + kk;
-            double* rb = row2[k & 1];
-            if (ty == kk) {
-                const double inv = 1.0 / S[k * SLD + k];
+            for (int c = 0; c < DB; ++c) a[c] = c <= lane ? S[i * SLD + c0 + c] : 0.0;
+            int bad = -1;  // first non-positive pivot (uniform across the warp); later steps run on 1
+            double* colj = Tm;  // column j of L, broadcast through shared memory
 #pragma unroll
-                for (int q2 = 0; q2 < 8; ++q2) {
-                    a[q][q2] *= inv;
-                    rb[tx + 16 * q2] = a[q][q2];
+            for (int j = 0; j < DB; ++j) {
+                double d = __shfl_sync(0xffffffffu, a[j], j);
+                if (!(d > 0.0)) {  // also catches NaN
+                    if (bad < 0) bad = j;
+                    d = 1.0;
                 }
+                const double r = recip_sqrt(d);
+                const double l = lane == j ? d * r : a[j] * r;  // L(i, j); zero above the diagonal
+                a[j] = l;
+                if (lane == j) rd[c0 + j] = r;
+                colj[lane] = l;
+                __syncwarp();
+#pragma unroll
+                for (int c = 0; c < DB; ++c) {
+                    if (c <= j) continue;
+                    if (lane >= c) a[c] = fma(-l, colj[c], a[c]);  // a(i, c) -= L(i, j) L(c, j)
+                }
+                __syncwarp();
             }
-            __syncthreads();
-            double xr[8];
-#pragma unroll
-            for (int q2 = 0; q2 < 8; ++q2) xr[q2] = rb[tx + 16 * q2];
-#pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                const int i = ty + 16 * r;
-                if (i > k) {
-                    const double l = S[i * SLD + k];
-#pragma unroll
-                    for (int q2 = 0; q2 < 8; ++q2) a[r][q2] = fma(-l, xr[q2], a[r][q2]);
+            if (bad >= 0) {
+                if (lane == 0) {
+                    record_first(info, (int)(g0 + c0 + bad + 1));
+                    *fail = 1;
                 }
+            } else {
+#pragma unroll
+                for (int c = 0; c < DB; ++c)
+                    if (c <= lane) S[i * SLD + c0 + c] = a[c];
             }
         }
+        __syncthreads();
+        if (*fail) return;
+        if (warp == 0) {  // 2a. inverse of the sub-block, column `lane` in registers
+            double x[DB];
+#pragma unroll
+            for (int q = 0; q < DB; ++q) x[q] = q == lane ? 1.0 : 0.0;
+#pragma unroll
+            for (int m = 0; m < DB; ++m) {
+                x[m] *= rd[c0 + m];
+#pragma unroll
+                for (int q = m + 1; q < DB; ++q) x[q] = fma(-S[(c0 + q) * SLD + c0 + m], x[m], x[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < DB; ++q)
+                if (q > lane) S[(c0 + lane) * SLD + c0 + q] = x[q];
+        } else if (tid - 32 < NB - c0 - DB) {  // 2b. one row below the sub-block per thread
+            const int i = c0 + DB + (tid - 32);
+            double r[DB];
+#pragma unroll
+            for (int c = 0; c < DB; ++c) r[c] = S[i * SLD + c0 + c];
+#pragma unroll
+            for (int j = 0; j < DB; ++j) {
+                r[j] *= rd[c0 + j];
+#pragma unroll
+                for (int c = j + 1; c < DB; ++c) r[c] = fma(-r[j], S[(c0 + c) * SLD + c0 + j], r[c]);
+            }
+#pragma unroll
+            for (int c = 0; c < DB; ++c) S[i * SLD + c0 + c] = r[c];
+        }
+        __syncthreads();
+        if (kb == 0) trailing_update<0>(S);  // 3.
+        else if (kb == 1) trailing_update<1>(S);
+        else if (kb == 2) trailing_update<2>(S);
+        __syncthreads();
     }
-#pragma unroll
-    for (int r = 0; r < 8; ++r)
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int i = ty + 16 * r, c = tx + 16 * q;
-            W[w_row_major ? i * NB + c : c * NB + i] = c <= i ? (T)a[r][q] : T(0);
-        }
+    // L back to global memory (lower part).
+    for (int e = tid; e < NB * NB; e += 256) {
+        const int i = rowmaj ? e / NB : e % NB, c = rowmaj ? e % NB : e / NB;
+        if (i < sz && c <= i) A(i, c) = (T)S[i * SLD + c];
+    }
+    __syncthreads();
+    // inv(L): the inverse's diagonal replaces L's, then 32-blocks -> 64-blocks (two merges,
+    // 128 threads each) -> the 128-block.
+    if (tid < NB) S[tid * SLD + tid] = rd[tid];
+    __syncthreads();
+    double* Th = Tm + (tid >= 128 ? 32 * 65 : 0);
+    inverse_merge<32, 128>(S, Th, tid >= 128 ? 64 : 0, tid & 127, 0);
+    __syncthreads();
+    inverse_merge<32, 128>(S, Th, tid >= 128 ? 64 : 0, tid & 127, 1);
+    __syncthreads();
+    inverse_merge<64, 256>(S, Tm, 0, tid, 0);
+    __syncthreads();
+    inverse_merge<64, 256>(S, Tm, 0, tid, 1);
+    __syncthreads();
+    for (int e = tid; e < NB * NB; e += 256) {
+        const int i = w_row_major ? e / NB : e % NB, c = w_row_major ? e % NB : e / NB;
+        const double v = S[c * SLD + i];
+        W[e] = (T)(i >= c ? v : 0.0);
+    }
 }
 
 template <class K>
@@ -260,7 +375,7 @@ int potrf_lower(int64_t n, View<T> A, int* info, cudaStream_t s) {
         tmp = static_cast<T*>(workspace(s, (size_t)n * NB * sizeof(T), 2));
         if (!tmp) return RC_ERR_ALLOC;
     }
-    RC_TRY(set_smem(potrf_diag<T>, kBlockSmem));
+    RC_TRY(set_smem(potrf_diag<T>, kDiagSmem));
     const View<const T> Wt = {W, NB, 1};  // inv(L_jj)^T
     // Outer panels of kOuter columns: inner 128-column blocks update only the rest of
     // their panel, and the trailing matrix gets one update of depth kOuter per panel, so
@@ -271,7 +386,7 @@ int potrf_lower(int64_t n, View<T> A, int* info, cudaStream_t s) {
         const int64_t w = (n - k0) < kOuter ? n - k0 : kOuter;
         for (int64_t j0 = k0; j0 < k0 + w; j0 += NB) {
             const int jb = (int)((k0 + w - j0) < NB ? k0 + w - j0 : NB);
-            potrf_diag<T><<<1, 256, kBlockSmem, s>>>(A.sub(j0, j0), jb, j0, W, info, false);
+            potrf_diag<T><<<1, 256, kDiagSmem, s>>>(A.sub(j0, j0), jb, j0, W, info, false);
             RC_TRY(check_launch());
             const int64_t rows = n - j0 - jb;
             if (rows <= 0) continue;
@@ -298,8 +413,8 @@ int potrf_lower(int64_t n, View<T> A, int* info, cudaStream_t s) {
 
 template <class T>
 int potrf_diag_block(View<T> A, int sz, int64_t g0, T* W, bool w_row_major, int* info, cudaStream_t s) {
-    RC_TRY(set_smem(potrf_diag<T>, kBlockSmem));
-    potrf_diag<T><<<1, 256, kBlockSmem, s>>>(A, sz, g0, W, info, w_row_major);
+    RC_TRY(set_smem(potrf_diag<T>, kDiagSmem));
+    potrf_diag<T><<<1, 256, kDiagSmem, s>>>(A, sz, g0, W, info, w_row_major);
     return check_launch();
 }
 
