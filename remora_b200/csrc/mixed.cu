@@ -545,7 +545,11 @@ int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* 
     auto add = [&](size_t x) { b += (x + 255) & ~size_t(255); };
     add((size_t)n * ldw * sizeof(float));               // W
     add((size_t)nblk * kNB * kNB * sizeof(float));      // diagonal-block inverses
-    if (prec == RC_PREC_BF16) add((size_t)n * ((ow + 63) / 64 * 64) * 2);  // BF16 panel
+    if (prec == RC_PREC_BF16) {
+        add((size_t)n * ((ow + 63) / 64 * 64) * 2);  // BF16 outer panels (two)
+        add((size_t)n * ((ow + 63) / 64 * 64) * 2);
+        add((size_t)n * kNB * 2);                    // BF16 128-column block
+    }
     add((size_t)n * sizeof(double));                    // s
     add((size_t)n * sizeof(double));                    // column sums
     for (int i = 0; i < 4; ++i) add((size_t)n * nrhs * sizeof(double));  // R, Z, P, Q
@@ -562,6 +566,22 @@ int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* 
 
 namespace {
 
+// One high-priority non-blocking stream per device for the factorisation's look-ahead
+// (kept for the life of the process).
+cudaStream_t lookahead_stream() {
+    static cudaStream_t streams[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!streams[dev]) {
+        int lo = 0, hi = 0;
+        if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) return nullptr;
+        cudaStream_t st = nullptr;
+        if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, hi) != cudaSuccess) return nullptr;
+        streams[dev] = st;
+    }
+    return streams[dev];
+}
+
 struct Mixed {
     int64_t n, nrhs, ldw, nblk;
     int prec;
@@ -570,7 +590,8 @@ struct Mixed {
     int64_t lda;
     float* W;
     float* Winv;
-    void* Pb;
+    void* Pb[2];  // BF16 outer panels, alternating
+    void* Pi;     // BF16 128-column block of the panel steps
     int64_t ldpb;
     double* sc;
     double* colsum;
@@ -584,45 +605,98 @@ struct Mixed {
     View<const double> Av() const { return {A, 1, lda}; }
     View<float> Wv() const { return {W, ldw, 1}; }
 
-    int factor(int outer, int* info) {
+    // The 128-column steps of one outer panel [k0, k0 + w), on stream st: factor (and
+    // invert) the diagonal block in FP64, solve the rows below it with that inverse on the
+    // TF32 tensor cores, update the rest of the panel's columns.
+    int panel_chain(int64_t k0, int64_t w, int* info, cudaStream_t st) {
         const View<float> Wm = Wv();
-        for (int64_t k0 = 0; k0 < n; k0 += outer) {
-            const int64_t w = (n - k0 < outer) ? n - k0 : outer;
-            for (int64_t j0 = k0; j0 < k0 + w; j0 += kNB) {
-                const int jb = (int)((k0 + w - j0) < kNB ? k0 + w - j0 : kNB);
-                float* Wb = Winv + (size_t)(j0 / kNB) * kNB * kNB;
-                RC_TRY(potrf_diag_block<float>(Wm.sub(j0, j0), jb, j0, Wb, true, info, s));
-                const int64_t rows = n - j0 - jb;
-                if (rows <= 0) continue;
-                View<float> Pj = Wm.sub(j0 + jb, j0);
-                // Panel solve in place: P <- P inv(L_jj)^T (TF32 tensor cores, one column tile).
-                RC_TRY(gemm_tc_kmajor(false, rows, jb, jb, 1.f, Pj.p, ldw, Wb, kNB, 0.f, Pj, kFull, 0, s, info, 128));
-                const int64_t cw = k0 + w - (j0 + jb);
-                if (cw <= 0) continue;
-                const void* op = Pj.p;
-                int64_t ldo = ldw;
-                if (prec == RC_PREC_BF16) {
-                    RC_TRY(pack_kmajor(rows, jb, View<const float>{Pj.p, Pj.rs, Pj.cs}, Pb, ldpb, true, s));
-                    op = Pb;
-                    ldo = ldpb;
-                }
-                RC_TRY(gemm_tc_kmajor(prec == RC_PREC_BF16, rows, cw, jb, -1.f, op, ldo, op, ldo, 1.f,
-                                      Wm.sub(j0 + jb, j0 + jb), kLower, 0, s, info));
-            }
-            const int64_t rows = n - k0 - w;
+        for (int64_t j0 = k0; j0 < k0 + w; j0 += kNB) {
+            const int jb = (int)((k0 + w - j0) < kNB ? k0 + w - j0 : kNB);
+            float* Wb = Winv + (size_t)(j0 / kNB) * kNB * kNB;
+            RC_TRY(potrf_diag_block<float>(Wm.sub(j0, j0), jb, j0, Wb, true, info, st));
+            const int64_t rows = n - j0 - jb;
             if (rows <= 0) continue;
-            View<float> Pk = Wm.sub(k0 + w, k0);
-            const void* op = Pk.p;
+            View<float> Pj = Wm.sub(j0 + jb, j0);
+            // Panel solve in place: P <- P inv(L_jj)^T (TF32 tensor cores, one column tile).
+            RC_TRY(gemm_tc_kmajor(false, rows, jb, jb, 1.f, Pj.p, ldw, Wb, kNB, 0.f, Pj, kFull, 0, st, info, 128));
+            const int64_t cw = k0 + w - (j0 + jb);
+            if (cw <= 0) continue;
+            const void* op = Pj.p;
             int64_t ldo = ldw;
             if (prec == RC_PREC_BF16) {
-                RC_TRY(pack_kmajor(rows, w, View<const float>{Pk.p, Pk.rs, Pk.cs}, Pb, ldpb, true, s));
-                op = Pb;
-                ldo = ldpb;
+                RC_TRY(pack_kmajor(rows, jb, View<const float>{Pj.p, Pj.rs, Pj.cs}, Pi, kNB, true, st));
+                op = Pi;
+                ldo = kNB;
             }
-            RC_TRY(gemm_tc_kmajor(prec == RC_PREC_BF16, rows, rows, w, -1.f, op, ldo, op, ldo, 1.f,
-                                  Wm.sub(k0 + w, k0 + w), kLower, 0, s, info));
+            RC_TRY(gemm_tc_kmajor(prec == RC_PREC_BF16, rows, cw, jb, -1.f, op, ldo, op, ldo, 1.f,
+                                  Wm.sub(j0 + jb, j0 + jb), kLower, 0, st, info));
         }
         return RC_SUCCESS;
+    }
+
+    // Blocked right-looking factorisation with a look-ahead of one outer panel. With panel
+    // p factored, the look-ahead stream (high priority) updates the columns of panel p + 1
+    // (T1) and factors that panel while the main stream applies panel p to everything to
+    // its right (T2, the bulk of the flops), so the latency-bound 128-column steps run in
+    // the shadow of the trailing update:
+    //   look-ahead: pack(p) -> rec(packed) -> wait(T2(p-1)) -> T1(p) -> chain(p + 1)
+    //   main:       wait(packed) -> T2(p) -> rec(T2(p))
+    // T1(p) and T2(p) write disjoint columns; T1(p) waits for T2(p - 1), whose columns
+    // include panel p + 1's. BF16 panels are packed into two alternating buffers.
+    int factor(int outer, int* info) {
+        const View<float> Wm = Wv();
+        cudaStream_t la = lookahead_stream();
+        if (!la) return RC_ERR_CUDA;
+        cudaEvent_t ev_fork, ev_packed, ev_t2, ev_join;
+        if (cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_packed, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_t2, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess)
+            return RC_ERR_CUDA;
+        struct Events {
+            cudaEvent_t e[4];
+            ~Events() { for (cudaEvent_t x : e) cudaEventDestroy(x); }
+        } guard{{ev_fork, ev_packed, ev_t2, ev_join}};
+        auto ok = [](cudaError_t e) { return e == cudaSuccess ? RC_SUCCESS : RC_ERR_CUDA; };
+        RC_TRY(ok(cudaEventRecord(ev_fork, s)));
+        RC_TRY(ok(cudaStreamWaitEvent(la, ev_fork, 0)));
+        RC_TRY(panel_chain(0, n < outer ? n : outer, info, la));
+        bool t2_pending = false;
+        for (int64_t p = 0, k0 = 0; k0 < n; ++p, k0 += outer) {
+            const int64_t w = (n - k0 < outer) ? n - k0 : outer;
+            const int64_t k1 = k0 + w, rows = n - k1;
+            if (rows <= 0) break;
+            View<float> Pk = Wm.sub(k1, k0);
+            const void* op = Pk.p;
+            int64_t ldo = ldw;
+            const bool bf16 = prec == RC_PREC_BF16;
+            if (bf16) {
+                op = Pb[p & 1];
+                ldo = ldpb;
+                RC_TRY(pack_kmajor(rows, w, View<const float>{Pk.p, Pk.rs, Pk.cs}, Pb[p & 1], ldpb, true, la));
+            }
+            RC_TRY(ok(cudaEventRecord(ev_packed, la)));
+            if (t2_pending) RC_TRY(ok(cudaStreamWaitEvent(la, ev_t2, 0)));
+            const int64_t w1 = rows < outer ? rows : outer;  // width of panel p + 1
+            // T1: rows [k1, n) x columns [k1, k1 + w1) on the look-ahead stream
+            RC_TRY(gemm_tc_kmajor(bf16, rows, w1, w, -1.f, op, ldo, op, ldo, 1.f, Wm.sub(k1, k1), kLower, 0, la, info));
+            // T2: rows and columns [k1 + w1, n) on the main stream
+            const int64_t r2 = rows - w1;
+            if (r2 > 0) {
+                const size_t esz = bf16 ? 2 : 4;
+                const void* op2 = static_cast<const char*>(op) + (size_t)w1 * ldo * esz;
+                RC_TRY(ok(cudaStreamWaitEvent(s, ev_packed, 0)));
+                RC_TRY(gemm_tc_kmajor(bf16, r2, r2, w, -1.f, op2, ldo, op2, ldo, 1.f, Wm.sub(k1 + w1, k1 + w1), kLower,
+                                      0, s, info));
+                RC_TRY(ok(cudaEventRecord(ev_t2, s)));
+                t2_pending = true;
+            } else {
+                t2_pending = false;
+            }
+            RC_TRY(panel_chain(k1, w1, info, la));
+        }
+        RC_TRY(ok(cudaEventRecord(ev_join, la)));
+        return ok(cudaStreamWaitEvent(s, ev_join, 0));
     }
 
     // Zout = M^-1 Rin = S L^-T L^-1 S Rin (FP64 in/out, FP32 triangular solves), on st.
@@ -734,7 +808,9 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     M.W = buf.take<float>((size_t)n * M.ldw);
     M.Winv = buf.take<float>((size_t)M.nblk * kNB * kNB);
     M.ldpb = (o.outer + 63) / 64 * 64;
-    M.Pb = prec == RC_PREC_BF16 ? static_cast<void*>(buf.take<uint16_t>((size_t)n * M.ldpb)) : nullptr;
+    for (int q = 0; q < 2; ++q)
+        M.Pb[q] = prec == RC_PREC_BF16 ? static_cast<void*>(buf.take<uint16_t>((size_t)n * M.ldpb)) : nullptr;
+    M.Pi = prec == RC_PREC_BF16 ? static_cast<void*>(buf.take<uint16_t>((size_t)n * kNB)) : nullptr;
     M.sc = buf.take<double>(n);
     M.colsum = buf.take<double>(n);
     M.R = buf.take<double>((size_t)n * nrhs);
