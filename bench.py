@@ -161,6 +161,18 @@ def run_reference_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(value: float, device=None) -> float:
+    """The largest of the ranks' values (the job's time is its slowest replica's); with no
+    process group, the value itself. Every rank must call it, in the same order."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -205,11 +217,7 @@ def run_ours(args) -> None:
         e1.record(stream)
         barrier()
     launches = lib.rc_launch_count() - launches0
-    t = e0.elapsed_time(e1) / 1e3
-    tmax = torch.tensor([t], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    t = float(tmax.item())
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3, dev)
     mixed_bwd = backward_error(A, X, B)
     status_ok = all(s == 0 for _, s in infos)
     last = infos[-1][0]
@@ -257,10 +265,7 @@ def run_ours(args) -> None:
             Xh.copy_(X, non_blocking=True)
         e1.record(stream)
         barrier()
-        te = torch.tensor([e0.elapsed_time(e1) / 1e3], device=dev, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        te = float(te.item())
+        te = max_over_ranks(e0.elapsed_time(e1) / 1e3, dev)
         e2e = {"value": world * args.steps * flops(n, nrhs) / te / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": n * n * 8 + n * nrhs * 8, "d2h_bytes_per_step": n * nrhs * 8,
                "ms_per_step": te / args.steps * 1e3}
@@ -299,6 +304,10 @@ def run_ours(args) -> None:
     syrk_flops = float(rows) * (rows + 1) * outer
     achieved = syrk_flops / tk / 1e12
     peak = peaks["bf16_tflops"] if prec else peaks["bf16_tflops"] / 2.0
+    # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu
+    # capture of the TF32 kernel at C = 8192 x 8192, depth 1024 (256.3 MB), scaled to this
+    # shape by the C area it reads and writes ((rows / 8192)^2); not captured for BF16.
+    traffic = None if prec else 256.3e6 * (rows / 8192.0) ** 2
     del P, C
     torch.cuda.empty_cache()
 
@@ -333,7 +342,9 @@ def run_ours(args) -> None:
             "speedup_vs_cusolver": tcus / (t / args.steps),
             "roofline": {"kernel": f"tc_gemm_kernel (lower SYRK {rows}x{rows}x{outer}, {args.precision})",
                          "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": "ncu DRAM bytes of the 8192 x 8192 x 1024 launch scaled by C area"
+                         if traffic else None,
                          "peak_source": ("bf16_tflops of " if prec else "bf16_tflops/2 (TF32 rate) of ")
                          + peaks.get("source", "?") + " peaks",
                          "algorithmic": "n(n+1)k flops per launch"},
