@@ -130,53 +130,47 @@ __global__ void col_xpby_kernel(int64_t n, int64_t c, const double* b, const dou
 
 // ---------------------------------------------------------------------------------------
 // Few-right-hand-side triangular solves with the FP32 factor (the CG preconditioner).
-// After the factorisation the lower triangle of W holds L and the strict upper triangle
-// is overwritten with L^T (W(i, j) = L(j, i) for j > i), so that both solve directions read
-// a contiguous ROW panel of W. Y holds the row-major inverses of the BS x BS diagonal
-// blocks (BS = 1024, built once per solve from the 128-block inverses of the
-// factorisation); block b occupies rows [b BS, (b + 1) BS) of the n x BS array Y. The
-// FP32 right-hand sides live in 64-column chunks, row-major inside a chunk (element
-// (i, j) of chunk q at q n 64 + i 64 + j, padding columns zero), so a K slice of a chunk
-// is one contiguous run. One block step is two launches of the same register-blocked
-// SIMT kernel:
-//   diag:   X_b = M_b R_b      M_b = inv(L_bb) (forward) or inv(L_bb)^T (backward)
-//   update: forward  R[r0+sz:] -= L[r0+sz:, r0:r0+sz] X_b   (L^T rows of the upper part)
-//           backward R[:r0]    -= L[r0:r0+sz, :r0]^T   X_b   (L rows of the lower part)
+// After the factorisation the strict lower triangle of W is truncated to TF32 in place and
+// the strict upper triangle receives the transpose (W(i, j) = L'(j, i) for j > i), so that
+// both solve directions read contiguous ROW segments of W, K-major for the tensor cores:
+//   forward  step b: R[r0+sz:]  -= L'[r0+sz:, r0:r0+sz] X_b   (rows of the lower part)
+//   backward step b: R[:r0]     -= L'[r0:r0+sz, :r0]^T  X_b   (rows of the upper part)
+// The preconditioner is therefore the fixed operator (L' L'^T)^-1 with L' = the factor's
+// diagonal BS x BS blocks (exact FP32, applied through their inverses Y) and its
+// off-diagonal blocks rounded down to TF32 -- symmetric and positive definite like
+// (L L^T)^-1 and as close to A^-1 as the TF32 factor itself. The vectors stay FP32: each
+// diagonal step writes X_b also as its exact TF32 split [X_hi; X_lo] (128 columns), and the
+// update runs on the tcgen05 tensor cores as one TF32 GEMM against that 128-row operand
+// whose two column halves are summed in the epilogue, i.e. L' times X to FP32 accuracy.
+// Y holds the row-major inverses of the BS x BS diagonal blocks (BS = 1024, built once
+// per solve from the 128-block inverses of the factorisation); block b occupies rows
+// [b BS, (b + 1) BS) of the n x BS array Y. Right-hand sides, solutions and the split
+// are column-major with leading dimension ldx (a multiple of 32), 64 columns per chunk
+// (padding columns zero).
 constexpr int RHS = 64;
 constexpr int BS = 1024;  // diagonal block of the preconditioner solves
 constexpr int UK = 32;    // K slice staged in shared memory
 
-// T = fl32(s .* R) in the chunked layout (R column-major, c columns), and back: Z = s .* T.
-// 32 x 32 tiles transposed through shared memory; grid (ceil(n/32), 2 ceil(c/64)).
-__global__ void to_f32_scaled_kernel(int64_t n, int64_t c, const double* s, const double* R, int64_t ldr, float* T) {
-    __shared__ float tile[32][33];
-    const int64_t i0 = (int64_t)blockIdx.x * 32, j0 = (int64_t)blockIdx.y * 32;
-    for (int r = threadIdx.y; r < 32; r += 8) {
-        const int64_t i = i0 + threadIdx.x, j = j0 + r;
-        tile[r][threadIdx.x] = (i < n && j < c) ? (float)(s[i] * R[i + j * ldr]) : 0.f;
-    }
-    __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += 8) {
-        const int64_t i = i0 + r, j = j0 + threadIdx.x;
-        if (i < n) T[(j / RHS) * n * RHS + i * RHS + j % RHS] = tile[threadIdx.x][r];
-    }
+__device__ __forceinline__ float tf32_hi(float v) { return __uint_as_float(__float_as_uint(v) & 0xFFFFE000u); }
+
+// T[:, j] = fl32(s .* R[:, j]) for j < c, zero for the padding columns up to gridDim.y;
+// and back: Z = s .* T.
+__global__ void to_f32_scaled_kernel(int64_t n, int64_t c, const double* s, const double* R, int64_t ldr, float* T,
+                                     int64_t ldx) {
+    const int64_t j = blockIdx.y;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        T[j * ldx + i] = j < c ? (float)(s[i] * R[i + j * ldr]) : 0.f;
 }
-__global__ void from_f32_scaled_kernel(int64_t n, int64_t c, const double* s, const float* T, double* Z, int64_t ldz) {
-    __shared__ float tile[32][33];
-    const int64_t i0 = (int64_t)blockIdx.x * 32, j0 = (int64_t)blockIdx.y * 32;
-    for (int r = threadIdx.y; r < 32; r += 8) {
-        const int64_t i = i0 + r, j = j0 + threadIdx.x;
-        tile[r][threadIdx.x] = i < n ? T[(j / RHS) * n * RHS + i * RHS + j % RHS] : 0.f;
-    }
-    __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += 8) {
-        const int64_t i = i0 + threadIdx.x, j = j0 + r;
-        if (i < n && j < c) Z[i + j * ldz] = s[i] * (double)tile[threadIdx.x][r];
-    }
+__global__ void from_f32_scaled_kernel(int64_t n, int64_t c, const double* s, const float* T, int64_t ldx, double* Z,
+                                       int64_t ldz) {
+    const int64_t j = blockIdx.y;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        Z[i + j * ldz] = s[i] * (double)T[j * ldx + i];
 }
 
-// W(i, j) = W(j, i) for j > i: the strict upper triangle receives L^T. 32 x 32 tiles: the
-// CTA of upper tile (bi, bj), bj >= bi, reads lower tile (bj, bi) and writes it transposed.
+// Strict lower triangle of W rounded down to TF32 in place and mirrored into the strict
+// upper triangle. 32 x 32 tiles: the CTA of upper tile (bi, bj), bj >= bi, reads lower tile
+// (bj, bi) into shared memory, then writes it back truncated and writes its transpose.
 __global__ void mirror_lower_kernel(int64_t n, float* W, int64_t ldw) {
     __shared__ float tile[32][33];
     const int64_t bi = blockIdx.y, bj = blockIdx.x;
@@ -186,40 +180,41 @@ __global__ void mirror_lower_kernel(int64_t n, float* W, int64_t ldw) {
         if (i < n && j <= i) tile[r][threadIdx.x] = W[i * ldw + j];
     }
     __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        const int64_t i = bj * 32 + r, j = bi * 32 + threadIdx.x;
+        if (i < n && j < i) W[i * ldw + j] = tf32_hi(tile[r][threadIdx.x]);
+    }
     for (int r = threadIdx.y; r < 32; r += 8) {  // upper tile rows bi*32 + r, columns bj*32 + tx
         const int64_t i = bi * 32 + r, j = bj * 32 + threadIdx.x;
-        if (j < n && j > i) W[i * ldw + j] = tile[threadIdx.x][r];
+        if (j < n && j > i) W[i * ldw + j] = tf32_hi(tile[threadIdx.x][r]);
     }
 }
 
-// Rows [row_begin, row_end) of the 64-column chunk Out: Out (=, or -=) A X, with
-// A(i, k) = A[i lda + k] (TRANS = false) or A[k lda + i] (TRANS = true), k < K, and X the
-// K x 64 row-major slice. NT threads in 8 column groups (columns 4 tx + {0..3} and
-// 32 + 4 tx + {0..3}) and NT / 8 row groups of TM rows: a CTA owns UM = NT TM / 8 rows.
-// K is split over the gridDim.y CTAs of a thread-block cluster (1, parts, 1); each takes
-// a contiguous run of UK-slices, staged in shared memory through registers (the next
-// slice is fetched while the current one is multiplied). The partial products are then
-// summed across the cluster through distributed shared memory in rank order (a
-// deterministic result), each CTA finishing UM / parts rows. Requires lda % 4 == 0, A,
-// X, Out 16-byte aligned, and for TRANS row_begin % 4 == 0.
-template <bool TRANS, bool ASSIGN, int TM, int NT>
-__global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t row_end, int K, const float* A,
-                                                      int64_t lda, const float* X, float* Out) {
-    constexpr int UM = NT * TM / 8;
-    constexpr int UAP = UM + 4;
-    constexpr int NA = UM * UK / 4 / NT;   // float4 of A per thread and slice (= TM)
-    constexpr int NX = UK * RHS / 4 / NT;  // float4 of X per thread and slice
-    static_assert(UK * UAP + UK * RHS >= UM * RHS, "the reduction reuses the staging buffers");
-    __shared__ __align__(16) float sm[UK * UAP + UK * RHS];
-    float* As = sm;               // As[k * UAP + i]
-    float* Xs = sm + UK * UAP;    // Xs[k * RHS + j]
+// Diagonal step X_b = M_b R_b for rows [0, sz) of one block: M_b(i, k) = Yb[i BS + k]
+// (TRANS = false, forward) or Yb[k BS + i] (backward), R_b the block's rows of the
+// right-hand sides. Writes X_b to Xp and its TF32 split to Xs (columns j and 64 + j).
+// 64 threads, 16-row tiles: 8 column groups (columns 4 tx + {0..3} and 32 + 4 tx + {0..3})
+// x 8 row pairs. K is split over the gridDim.y CTAs of a thread-block cluster (1, parts,
+// 1), each taking a contiguous run of UK-slices staged in shared memory through registers
+// (the next slice is fetched while the current one is multiplied); the partial tiles are
+// summed through distributed shared memory in rank order (deterministic), each CTA
+// finishing 16 / parts rows.
+template <bool TRANS>
+__global__ void __launch_bounds__(64) pre_diag_kernel(int sz, const float* Yb, const float* Rb, int64_t ldx, float* Xp,
+                                                      float* Xs) {
+    constexpr int NT = 64, TM = 2, UM = 16, UAP = UM + 4, XP = RHS + 4;
+    constexpr int NA = UM * UK / 4 / NT;   // float4 of M per thread and slice (2)
+    constexpr int NX = UK * RHS / 4 / NT;  // float4 of R per thread and slice (8)
+    __shared__ __align__(16) float sm[UK * UAP + UK * XP];
+    float* As = sm;             // As[k * UAP + i]
+    float* Rs = sm + UK * UAP;  // Rs[k * XP + j]
     const int tid = threadIdx.x;
-    const int64_t i0 = row_begin + (int64_t)blockIdx.x * UM;
+    const int i0 = blockIdx.x * UM;
     const int ty = tid / 8, tx = tid % 8;
     const int parts = gridDim.y, part = blockIdx.y;
-    const int kper = ((K + UK - 1) / UK + parts - 1) / parts * UK;  // whole slices per rank
-    const int kb = part * kper < K ? part * kper : K;
-    const int ke = kb + kper < K ? kb + kper : K;
+    const int kper = ((sz + UK - 1) / UK + parts - 1) / parts * UK;  // whole slices per rank
+    const int kb = part * kper < sz ? part * kper : sz;
+    const int ke = kb + kper < sz ? kb + kper : sz;
     float4 a_reg[NA], x_reg[NX];
     auto fetch = [&](int k0) {
 #pragma unroll
@@ -228,10 +223,9 @@ __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t
             float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
             if (!TRANS) {  // row ii, k = 4 kq .. 4 kq + 3
                 const int ii = e % UM, kq = e / UM;
-                const int64_t gi = i0 + ii;
-                const int k = k0 + 4 * kq;
-                if (gi < row_end) {
-                    const float* src = A + gi * lda + k;
+                const int gi = i0 + ii, k = k0 + 4 * kq;
+                if (gi < sz) {
+                    const float* src = Yb + (int64_t)gi * BS + k;
                     if (k + 3 < ke) {
                         v = *reinterpret_cast<const float4*>(src);
                     } else {
@@ -242,26 +236,34 @@ __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t
                 }
             } else {       // row k, rows of the tile 4 g4 .. 4 g4 + 3
                 const int g4 = e % (UM / 4), k = k0 + e / (UM / 4);
-                const int64_t gi = i0 + 4 * g4;
+                const int gi = i0 + 4 * g4;
                 if (k < ke) {
-                    const float* src = A + (int64_t)k * lda + gi;
-                    if (gi + 3 < row_end) {
+                    const float* src = Yb + (int64_t)k * BS + gi;
+                    if (gi + 3 < sz) {
                         v = *reinterpret_cast<const float4*>(src);
                     } else {
-                        if (gi < row_end) v.x = src[0];
-                        if (gi + 1 < row_end) v.y = src[1];
-                        if (gi + 2 < row_end) v.z = src[2];
+                        if (gi < sz) v.x = src[0];
+                        if (gi + 1 < sz) v.y = src[1];
+                        if (gi + 2 < sz) v.z = src[2];
                     }
                 }
             }
             a_reg[q] = v;
         }
 #pragma unroll
-        for (int q = 0; q < NX; ++q) {
+        for (int q = 0; q < NX; ++q) {  // column j, rows k .. k + 3 (column-major R)
             const int e = tid + NT * q;
-            const int k = k0 + e / (RHS / 4), c4 = e % (RHS / 4);
-            x_reg[q] = k < ke ? *reinterpret_cast<const float4*>(X + (int64_t)k * RHS + 4 * c4)
-                              : make_float4(0.f, 0.f, 0.f, 0.f);
+            const int k = k0 + 4 * (e % (UK / 4)), j = e / (UK / 4);
+            const float* src = Rb + (int64_t)j * ldx + k;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k + 3 < ke) {
+                v = *reinterpret_cast<const float4*>(src);
+            } else {
+                if (k < ke) v.x = src[0];
+                if (k + 1 < ke) v.y = src[1];
+                if (k + 2 < ke) v.z = src[2];
+            }
+            x_reg[q] = v;
         }
     };
     auto stage = [&]() {
@@ -282,7 +284,11 @@ __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t
 #pragma unroll
         for (int q = 0; q < NX; ++q) {
             const int e = tid + NT * q;
-            *reinterpret_cast<float4*>(&Xs[(e / (RHS / 4)) * RHS + 4 * (e % (RHS / 4))]) = x_reg[q];
+            const int k = 4 * (e % (UK / 4)), j = e / (UK / 4);
+            Rs[(k + 0) * XP + j] = x_reg[q].x;
+            Rs[(k + 1) * XP + j] = x_reg[q].y;
+            Rs[(k + 2) * XP + j] = x_reg[q].z;
+            Rs[(k + 3) * XP + j] = x_reg[q].w;
         }
     };
     float acc[TM][8];
@@ -297,47 +303,36 @@ __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t
         if (k0 + UK < ke) fetch(k0 + UK);
 #pragma unroll 4
         for (int k = 0; k < UK; ++k) {  // slices past ke are zero-filled
-            float av[TM];
-            if constexpr (TM % 4 == 0) {
-#pragma unroll
-                for (int u = 0; u < TM; u += 4) {
-                    const float4 t = *reinterpret_cast<const float4*>(&As[k * UAP + TM * ty + u]);
-                    av[u] = t.x; av[u + 1] = t.y; av[u + 2] = t.z; av[u + 3] = t.w;
-                }
-            } else {
-#pragma unroll
-                for (int u = 0; u < TM; ++u) av[u] = As[k * UAP + TM * ty + u];
-            }
-            const float4 x0 = *reinterpret_cast<const float4*>(&Xs[k * RHS + 4 * tx]);
-            const float4 x1 = *reinterpret_cast<const float4*>(&Xs[k * RHS + 32 + 4 * tx]);
+            const float a0 = As[k * UAP + TM * ty], a1 = As[k * UAP + TM * ty + 1];
+            const float4 x0 = *reinterpret_cast<const float4*>(&Rs[k * XP + 4 * tx]);
+            const float4 x1 = *reinterpret_cast<const float4*>(&Rs[k * XP + 32 + 4 * tx]);
             const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
 #pragma unroll
-            for (int u = 0; u < TM; ++u)
-#pragma unroll
-                for (int v = 0; v < 8; ++v) acc[u][v] = fmaf(av[u], xv[v], acc[u][v]);
+            for (int v = 0; v < 8; ++v) {
+                acc[0][v] = fmaf(a0, xv[v], acc[0][v]);
+                acc[1][v] = fmaf(a1, xv[v], acc[1][v]);
+            }
         }
         __syncthreads();
     }
-    auto emit = [&](int64_t gi, int col, float4 v) {  // Out[gi, col..col+3] (=, -=) v
-        float4* o = reinterpret_cast<float4*>(Out + gi * RHS + col);
-        if (!ASSIGN) {
-            const float4 p = *o;
-            v = make_float4(p.x - v.x, p.y - v.y, p.z - v.z, p.w - v.w);
-        }
-        *o = v;
+    auto emit = [&](int gi, int j, float v) {  // X_b(gi, j) and its split
+        const float h = tf32_hi(v);
+        Xp[(int64_t)j * ldx + gi] = v;
+        Xs[(int64_t)j * ldx + gi] = h;
+        Xs[(int64_t)(j + RHS) * ldx + gi] = v - h;
     };
     if (parts == 1) {
 #pragma unroll
         for (int u = 0; u < TM; ++u) {
-            const int64_t gi = i0 + TM * ty + u;
-            if (gi >= row_end) continue;
-            emit(gi, 4 * tx, make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]));
-            emit(gi, 32 + 4 * tx, make_float4(acc[u][4], acc[u][5], acc[u][6], acc[u][7]));
+            const int gi = i0 + TM * ty + u;
+            if (gi >= sz) continue;
+#pragma unroll
+            for (int v = 0; v < 8; ++v) emit(gi, (v < 4 ? 4 * tx : 32 + 4 * tx) + (v & 3), acc[u][v]);
         }
         return;
     }
-    // Cluster reduction: partial tile (UM x 64, row-major) in this CTA's shared memory,
-    // then rank p sums rows [p UM / parts, (p + 1) UM / parts) over ranks 0..parts-1.
+    // Cluster reduction: partial tile (16 x 64, row-major) in this CTA's shared memory,
+    // then rank p sums rows [p 16 / parts, (p + 1) 16 / parts) over ranks 0..parts-1.
 #pragma unroll
     for (int u = 0; u < TM; ++u) {
         float* r = sm + (TM * ty + u) * RHS;
@@ -347,41 +342,32 @@ __global__ void __launch_bounds__(NT) blk_gemm_kernel(int64_t row_begin, int64_t
     cg::cluster_group cluster = cg::this_cluster();
     cluster.sync();
     const int rows_per = UM / parts;
-    for (int e = tid; e < rows_per * (RHS / 4); e += NT) {
-        const int row = part * rows_per + e / (RHS / 4), col = 4 * (e % (RHS / 4));
-        float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int q = 0; q < parts; ++q) {
-            const float4 t = *reinterpret_cast<const float4*>(cluster.map_shared_rank(sm, q) + row * RHS + col);
-            sum.x += t.x; sum.y += t.y; sum.z += t.z; sum.w += t.w;
-        }
-        if (i0 + row < row_end) emit(i0 + row, col, sum);
+    for (int e = tid; e < rows_per * RHS; e += NT) {
+        const int row = part * rows_per + e / RHS, col = e % RHS;
+        float sum = 0.f;
+        for (int q = 0; q < parts; ++q) sum += cluster.map_shared_rank(sm, q)[row * RHS + col];
+        if (i0 + row < sz) emit(i0 + row, col, sum);
     }
     cluster.sync();  // the other ranks may still read this CTA's partial tile
 }
 
-constexpr int kDiagTM = 2, kDiagNT = 64;  // 16-row tiles for the diagonal steps
-constexpr int kUpdTM = 8, kUpdNT = 64;    // 64-row tiles for the updates
-
 // Split K over a cluster of up to 8 CTAs so that the launch fills about one wave of
-// resident CTAs (slots = SMs x CTAs per SM) with at least two UK-slices per CTA.
-template <bool TRANS, bool ASSIGN, int TM, int NT>
-int launch_blk(int64_t rb, int64_t re, int K, const float* A, int64_t lda, const float* X, float* Out,
-               cudaStream_t st) {
-    constexpr int UM = NT * TM / 8;
+// resident CTAs with at least two UK-slices per CTA.
+template <bool TRANS>
+int launch_pre_diag(int sz, const float* Yb, const float* Rb, int64_t ldx, float* Xp, float* Xs, cudaStream_t st) {
     static int slots = 0;
     if (slots == 0) {
         int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, blk_gemm_kernel<TRANS, ASSIGN, TM, NT>, NT, 0) !=
-            cudaSuccess)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pre_diag_kernel<TRANS>, 64, 0) != cudaSuccess)
             return RC_ERR_CUDA;
         slots = (per_sm > 0 ? per_sm : 1) * sm_count();
     }
-    const int64_t tiles = (re - rb + UM - 1) / UM;
+    const int tiles = (sz + 15) / 16;
     int parts = 1;
-    while (parts < 8 && tiles * parts * 2 <= slots && K >= parts * 2 * 2 * UK) parts *= 2;
+    while (parts < 8 && tiles * parts * 2 <= slots && sz >= parts * 2 * 2 * UK) parts *= 2;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)tiles, (unsigned)parts, 1);
-    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.blockDim = dim3(64, 1, 1);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -390,17 +376,18 @@ int launch_blk(int64_t rb, int64_t re, int K, const float* A, int64_t lda, const
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (cudaLaunchKernelEx(&cfg, blk_gemm_kernel<TRANS, ASSIGN, TM, NT>, rb, re, K, A, lda, X, Out) != cudaSuccess)
-        return RC_ERR_CUDA;
+    if (cudaLaunchKernelEx(&cfg, pre_diag_kernel<TRANS>, sz, Yb, Rb, ldx, Xp, Xs) != cudaSuccess) return RC_ERR_CUDA;
     return check_launch();
 }
 
-// Solve L X = R (bwd = false) or L^T X = R (bwd = true) for one 64-column chunk; R is
-// consumed (updated in place), X receives the solution. W holds L below and L^T above
-// the diagonal.
-int trsm_few(bool bwd, int64_t n, const float* W, int64_t ldw, const float* Y, float* R, float* X, cudaStream_t st) {
-    if (ldw % 4 != 0 || reinterpret_cast<uintptr_t>(W) % 16 != 0 || reinterpret_cast<uintptr_t>(Y) % 16 != 0 ||
-        reinterpret_cast<uintptr_t>(R) % 16 != 0 || reinterpret_cast<uintptr_t>(X) % 16 != 0)
+// Solve L' X = R (bwd = false) or L'^T X = R (bwd = true) for one 64-column chunk
+// (column-major, ld ldx): R is consumed (updated in place), X receives the solution, S
+// (128 columns) holds each step's TF32 split of X_b.
+int trsm_few(bool bwd, int64_t n, const float* W, int64_t ldw, const float* Y, float* R, float* X, float* S,
+             int64_t ldx, cudaStream_t st) {
+    if (ldw % 4 != 0 || ldx % 4 != 0 || reinterpret_cast<uintptr_t>(W) % 16 != 0 ||
+        reinterpret_cast<uintptr_t>(Y) % 16 != 0 || reinterpret_cast<uintptr_t>(R) % 16 != 0 ||
+        reinterpret_cast<uintptr_t>(X) % 16 != 0 || reinterpret_cast<uintptr_t>(S) % 16 != 0)
         return RC_ERR_INVALID_ARGUMENT;
     const int64_t nblk = (n + BS - 1) / BS;
     for (int64_t step = 0; step < nblk; ++step) {
@@ -408,16 +395,13 @@ int trsm_few(bool bwd, int64_t n, const float* W, int64_t ldw, const float* Y, f
         const int64_t r0 = b * BS;
         const int sz = (int)((n - r0) < BS ? n - r0 : BS);
         const float* Yb = Y + r0 * BS;
-        const float* Rb = R + r0 * RHS;
-        float* Xb = X + r0 * RHS;
-        const float* Wp = W + r0 * ldw;  // row panel [r0, r0 + sz)
-        if (bwd) {
-            RC_TRY(launch_blk<true, true, kDiagTM, kDiagNT>(0, sz, sz, Yb, BS, Rb, Xb, st));
-            if (r0 > 0) RC_TRY(launch_blk<true, false, kUpdTM, kUpdNT>(0, r0, sz, Wp, ldw, Xb, R, st));
-        } else {
-            RC_TRY(launch_blk<false, true, kDiagTM, kDiagNT>(0, sz, sz, Yb, BS, Rb, Xb, st));
-            if (r0 + sz < n) RC_TRY(launch_blk<true, false, kUpdTM, kUpdNT>(r0 + sz, n, sz, Wp, ldw, Xb, R, st));
-        }
+        if (bwd) RC_TRY(launch_pre_diag<true>(sz, Yb, R + r0, ldx, X + r0, S + r0, st));
+        else RC_TRY(launch_pre_diag<false>(sz, Yb, R + r0, ldx, X + r0, S + r0, st));
+        // rows [rb, re) of R -= W[rows, r0 : r0 + sz] (X_hi + X_lo)
+        const int64_t rb = bwd ? 0 : r0 + sz, re = bwd ? r0 : n;
+        if (re > rb)
+            RC_TRY(gemm_tc_fold_kmajor(re - rb, sz, -1.f, W + rb * ldw + r0, ldw, S + r0, ldx, 1.f,
+                                       View<float>{R + rb, 1, ldx}, st));
     }
     return RC_SUCCESS;
 }
@@ -553,9 +537,10 @@ int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* 
     add((size_t)n * sizeof(double));                    // s
     add((size_t)n * sizeof(double));                    // column sums
     for (int i = 0; i < 4; ++i) add((size_t)n * nrhs * sizeof(double));  // R, Z, P, Q
-    const size_t chunked = (size_t)n * ((nrhs + RHS - 1) / RHS) * RHS;  // 64-column chunks
+    const size_t chunked = (size_t)ldw * ((nrhs + RHS - 1) / RHS) * RHS;  // 64-column chunks, ld ldw
     add(chunked * sizeof(float));                       // FP32 right-hand side of the preconditioner
     add(chunked * sizeof(float));                       // FP32 intermediate of the preconditioner
+    add((size_t)ldw * 2 * RHS * sizeof(float));         // TF32 split of one solution block
     add((size_t)kNB * nrhs * sizeof(float));            // TRSM tile buffer
     add((size_t)((n + BS - 1) / BS) * BS * BS * sizeof(float));      // BS-block inverses
     add((size_t)((n + BS - 1) / BS) * BS * BS / 2 * sizeof(float));  // their scratch
@@ -596,8 +581,10 @@ struct Mixed {
     double* sc;
     double* colsum;
     double *R, *Z, *P, *Q;
-    float* T32;
-    float* T32b;
+    float* T32;   // FP32 right-hand sides / solutions of the preconditioner (ld ldv)
+    float* T32b;  // its intermediate
+    float* T32s;  // TF32 split of one block of the solution (128 columns)
+    int64_t ldv;
     float* Y;  // BS-block inverses
     float* Tinv;
     float* tmp;
@@ -702,16 +689,16 @@ struct Mixed {
     // Zout = M^-1 Rin = S L^-T L^-1 S Rin (FP64 in/out, FP32 triangular solves), on st.
     int precond_on(const double* Rin, int64_t ldr, double* Zout, int64_t ldz, cudaStream_t st) {
         const int64_t nch = (nrhs + RHS - 1) / RHS;  // 64-column chunks
-        const dim3 g(ceil_div(n, 32), (unsigned)(2 * nch)), tb(32, 8);
-        to_f32_scaled_kernel<<<g, tb, 0, st>>>(n, nrhs, sc, Rin, ldr, T32);
+        const dim3 g(ceil_div(n, 256) < 128u ? ceil_div(n, 256) : 128u, (unsigned)(nch * RHS));
+        to_f32_scaled_kernel<<<g, 256, 0, st>>>(n, nrhs, sc, Rin, ldr, T32, ldv);
         RC_TRY(check_launch());
         for (int64_t q = 0; q < nch; ++q) {
-            float* R1 = T32 + q * n * RHS;
-            float* R2 = T32b + q * n * RHS;
-            RC_TRY(trsm_few(false, n, W, ldw, Y, R1, R2, st));  // R2 = L^-1 R1
-            RC_TRY(trsm_few(true, n, W, ldw, Y, R2, R1, st));   // R1 = L^-T R2
+            float* R1 = T32 + q * RHS * ldv;
+            float* R2 = T32b + q * RHS * ldv;
+            RC_TRY(trsm_few(false, n, W, ldw, Y, R1, R2, T32s, ldv, st));  // R2 = L'^-1 R1
+            RC_TRY(trsm_few(true, n, W, ldw, Y, R2, R1, T32s, ldv, st));   // R1 = L'^-T R2
         }
-        from_f32_scaled_kernel<<<g, tb, 0, st>>>(n, nrhs, sc, T32, Zout, ldz);
+        from_f32_scaled_kernel<<<dim3(g.x, (unsigned)nrhs), 256, 0, st>>>(n, nrhs, sc, T32, ldv, Zout, ldz);
         return check_launch();
     }
     int precond(const double* Rin, int64_t ldr, double* Zout, int64_t ldz) {
@@ -817,8 +804,10 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     M.Z = buf.take<double>((size_t)n * nrhs);
     M.P = buf.take<double>((size_t)n * nrhs);
     M.Q = buf.take<double>((size_t)n * nrhs);
-    M.T32 = buf.take<float>((size_t)n * ((nrhs + RHS - 1) / RHS) * RHS);
-    M.T32b = buf.take<float>((size_t)n * ((nrhs + RHS - 1) / RHS) * RHS);
+    M.ldv = (n + 31) / 32 * 32;
+    M.T32 = buf.take<float>((size_t)M.ldv * ((nrhs + RHS - 1) / RHS) * RHS);
+    M.T32b = buf.take<float>((size_t)M.ldv * ((nrhs + RHS - 1) / RHS) * RHS);
+    M.T32s = buf.take<float>((size_t)M.ldv * 2 * RHS);
     M.tmp = buf.take<float>((size_t)kNB * nrhs);
     M.Y = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS);
     M.Tinv = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS / 2);

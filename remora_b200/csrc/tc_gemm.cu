@@ -43,7 +43,9 @@ struct TcCfg {
     static constexpr size_t SMEM = (size_t)STAGES * (A_BYTES + B_BYTES) + 1024 + 256;
 };
 
-template <int BN, bool BF16>
+// FOLD (BN = 128): the product's columns j and j + 64 are summed into column j of C (an
+// m x 64 result from a 128-row B = [B_hi; B_lo], the two halves of an exact TF32 split).
+template <int BN, bool BF16, bool FOLD = false>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int64_t M,
                    int64_t N, int64_t K, float alpha, float beta, View<float> C, Mask mask, int64_t off,
@@ -143,9 +145,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const bool row_ok = i < M;
             const bool vec = C.cs == 1 && (C.rs % 4 == 0) && (reinterpret_cast<uintptr_t>(C.p) % 16 == 0);
 #pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 16) {
+            for (int c0 = 0; c0 < (FOLD ? BN / 2 : BN); c0 += 16) {
                 float v[16];
                 tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+                if (FOLD) {
+                    float w[16];
+                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(c0 + BN / 2), w);
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) v[u] += w[u];
+                }
                 if (!row_ok) continue;
                 const int64_t j0 = n0 + c0;
                 if (vec && j0 + 15 < N && keep(mask, off, i, j0 + 15) && keep(mask, off, i, j0)) {
@@ -236,17 +244,17 @@ bool make_tmap(CUtensorMap* tm, const void* base, bool bf16, int64_t rows, int64
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int BN, bool BF16>
+template <int BN, bool BF16, bool FOLD = false>
 int launch_tc(const CUtensorMap& ta, const CUtensorMap& tb, int64_t m, int64_t n, int64_t k, float alpha, float beta,
               View<float> C, Mask mask, int64_t off, cudaStream_t s, const int* abort) {
     const size_t smem = TcCfg<BN>::SMEM;
-    if (cudaFuncSetAttribute(tc_gemm_kernel<BN, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(tc_gemm_kernel<BN, BF16, FOLD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
         return RC_ERR_CUDA;
-    dim3 grid(ceil_div(n, BN), ceil_div(m, 128));
+    dim3 grid(FOLD ? 1u : ceil_div(n, BN), ceil_div(m, 128));
     if (grid.y > 65535) return RC_ERR_NOT_SUPPORTED;
-    tc_gemm_kernel<BN, BF16><<<grid, TC_THREADS, smem, s>>>(ta, tb, m, n, k, alpha, beta, C, mask, off, abort,
-                                                            error_word(), wait_limit_ns());
+    tc_gemm_kernel<BN, BF16, FOLD><<<grid, TC_THREADS, smem, s>>>(ta, tb, m, n, k, alpha, beta, C, mask, off, abort,
+                                                                  error_word(), wait_limit_ns());
     return check_launch();
 }
 
@@ -271,6 +279,18 @@ int gemm_tc_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, cons
     }
     return bn == 256 ? launch_tc<256, false>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort)
                      : launch_tc<128, false>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort);
+}
+
+int gemm_tc_fold_kmajor(int64_t m, int64_t k, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
+                        float beta, View<float> C, cudaStream_t s, const int* abort) {
+    if (m <= 0) return RC_SUCCESS;
+    if (k <= 0 || (reinterpret_cast<uintptr_t>(A) % 16) || (reinterpret_cast<uintptr_t>(B) % 16) ||
+        ((lda * 4) % 16) || ((ldb * 4) % 16) || m > (int64_t)INT32_MAX || k > (int64_t)INT32_MAX)
+        return RC_ERR_NOT_SUPPORTED;
+    CUtensorMap ta, tb;
+    if (!make_tmap(&ta, A, false, m, k, lda, 128) || !make_tmap(&tb, B, false, 128, k, ldb, 128))
+        return RC_ERR_NOT_SUPPORTED;
+    return launch_tc<128, false, true>(ta, tb, m, 64, k, alpha, beta, C, kFull, 0, s, abort);
 }
 
 // One warp waits, bounded, on an mbarrier phase that nothing completes: exercises the

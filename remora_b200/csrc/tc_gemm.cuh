@@ -12,6 +12,12 @@ int gemm_tc_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, cons
                    const void* B, int64_t ldb, float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s,
                    const int* abort = nullptr, int bn = 0);
 
+// C (m x 64) = alpha * (A B^T folded) + beta * C for a 128-row K-major B = [B_hi; B_lo]:
+// column j of the product is A B_hi(j)^T + A B_lo(j)^T, i.e. A times B_hi + B_lo with
+// B's TF32 split exact. TF32 products, FP32 accumulation.
+int gemm_tc_fold_kmajor(int64_t m, int64_t k, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
+                        float beta, View<float> C, cudaStream_t s, const int* abort = nullptr);
+
 // Copy rows x K of X into a K-major buffer (row stride ldd), as FP32 or rounded to BF16.
 int pack_kmajor(int64_t rows, int64_t K, View<const float> X, void* dst, int64_t ldd, bool bf16, cudaStream_t s);
 
