@@ -35,9 +35,11 @@ using namespace tc;
 constexpr int KB_BYTES = 128;  // K extent of one pipeline stage, in bytes (one swizzle row)
 constexpr int TC_THREADS = 192;
 
-template <int BN>
+template <int BN, bool FOLD = false>
 struct TcCfg {
-    static constexpr int STAGES = BN == 256 ? 4 : 6;
+    // The folded skinny update runs two CTAs per SM (3 stages each): its launches often
+    // have more row tiles than SMs, and a second CTA overlaps one CTA's fill and epilogue.
+    static constexpr int STAGES = FOLD ? 3 : (BN == 256 ? 4 : 6);
     static constexpr int A_BYTES = 128 * KB_BYTES;
     static constexpr int B_BYTES = BN * KB_BYTES;
     static constexpr size_t SMEM = (size_t)STAGES * (A_BYTES + B_BYTES) + 1024 + 256;
@@ -46,11 +48,11 @@ struct TcCfg {
 // FOLD (BN = 128): the product's columns j and j + 64 are summed into column j of C (an
 // m x 64 result from a 128-row B = [B_hi; B_lo], the two halves of an exact TF32 split).
 template <int BN, bool BF16, bool FOLD = false>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(TC_THREADS, FOLD ? 2 : 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int64_t M,
                    int64_t N, int64_t K, float alpha, float beta, View<float> C, Mask mask, int64_t off,
                    const int* abort, int* err, uint64_t limit_ns) {
-    using Cfg = TcCfg<BN>;
+    using Cfg = TcCfg<BN, FOLD>;
     constexpr int STAGES = Cfg::STAGES;
     constexpr int KB_ELEMS = KB_BYTES / (BF16 ? 2 : 4);
     constexpr int MMAS_PER_STAGE = KB_BYTES / 32;  // each MMA consumes 32 bytes of K
@@ -136,6 +138,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
     } else {
         const int q = warp & 3;  // TMEM lane quadrant this warp may access
+        // FOLD: the rows of C this thread finishes are read while the main loop runs.
+        float cpre[FOLD ? BN / 2 : 1];
+        if constexpr (FOLD) {
+            const int64_t i = m0 + 32 * q + lane;
+#pragma unroll
+            for (int j = 0; j < BN / 2; ++j) cpre[j] = (beta != 0.f && i < M && j < N) ? C(i, j) : 0.f;
+        }
         const bool ok = mbar_wait_bounded(done, 0, stop, limit_ns);
         if (!ok) raise_stop(stop, err);
         tc_fence_after();
@@ -144,16 +153,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int64_t i = m0 + 32 * q + lane;
             const bool row_ok = i < M;
             const bool vec = C.cs == 1 && (C.rs % 4 == 0) && (reinterpret_cast<uintptr_t>(C.p) % 16 == 0);
+            if constexpr (FOLD) {
+#pragma unroll
+                for (int c0 = 0; c0 < BN / 2; c0 += 16) {
+                    float v[16], w[16];
+                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(c0 + BN / 2), w);
+                    if (!row_ok) continue;
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        const int j = c0 + u;
+                        if (j < N) C(i, j) = fmaf(beta, cpre[j], alpha * (v[u] + w[u]));
+                    }
+                }
+            }
 #pragma unroll 1
-            for (int c0 = 0; c0 < (FOLD ? BN / 2 : BN); c0 += 16) {
+            for (int c0 = 0; c0 < (FOLD ? 0 : BN); c0 += 16) {
                 float v[16];
                 tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
-                if (FOLD) {
-                    float w[16];
-                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(c0 + BN / 2), w);
-#pragma unroll
-                    for (int u = 0; u < 16; ++u) v[u] += w[u];
-                }
                 if (!row_ok) continue;
                 const int64_t j0 = n0 + c0;
                 if (vec && j0 + 15 < N && keep(mask, off, i, j0 + 15) && keep(mask, off, i, j0)) {
@@ -247,7 +264,7 @@ bool make_tmap(CUtensorMap* tm, const void* base, bool bf16, int64_t rows, int64
 template <int BN, bool BF16, bool FOLD = false>
 int launch_tc(const CUtensorMap& ta, const CUtensorMap& tb, int64_t m, int64_t n, int64_t k, float alpha, float beta,
               View<float> C, Mask mask, int64_t off, cudaStream_t s, const int* abort) {
-    const size_t smem = TcCfg<BN>::SMEM;
+    const size_t smem = TcCfg<BN, FOLD>::SMEM;
     if (cudaFuncSetAttribute(tc_gemm_kernel<BN, BF16, FOLD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
         return RC_ERR_CUDA;
