@@ -259,14 +259,24 @@ int launch_dmma(int64_t m, int64_t n, int64_t k, double alpha, View<const double
         cudaSuccess)
         return RC_ERR_CUDA;
     dim3 grid(ceil_div(n, BN), ceil_div(m, DM));
-    // Too few output tiles to fill the GPU and a long K: split K into slices.
-    const int64_t tiles = (int64_t)grid.x * grid.y, sms = sm_count();
+    // Long K: split it into nz slices when that packs the CTAs into the GPU's resident
+    // slots with less wave quantisation -- nz minimises ceil(tiles nz / slots) / nz (the
+    // time in units of one full-K tile) plus a small charge per slice for the reduction.
+    static int per_sm = 0;
+    if (per_sm == 0 &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gemm_dmma_f64<AK, BK, BN>, 256, smem) != cudaSuccess)
+        return RC_ERR_CUDA;
+    const int64_t tiles = (int64_t)grid.x * grid.y, slots = (int64_t)(per_sm > 0 ? per_sm : 1) * sm_count();
     int nz = 1;
-    if (mask == kFull && k >= 2048 && tiles < sms) {
-        nz = (int)((2 * sms + tiles - 1) / tiles);
-        nz = nz > 16 ? 16 : nz;
-        const int64_t maxz = k / 512;
-        if (nz > maxz) nz = (int)maxz;
+    if (mask == kFull && k >= 2048 && tiles < 4 * slots) {  // few waves: quantisation matters
+        double best = 1e30;
+        for (int z = 1; z <= 8 && (int64_t)z * 1024 <= k; ++z) {
+            const double cost = (double)((tiles * z + slots - 1) / slots) / z + 0.01 * (z - 1);
+            if (cost < best - 1e-9) {
+                best = cost;
+                nz = z;
+            }
+        }
     }
     if (nz > 1) {
         const int64_t kchunk = ((k + nz - 1) / nz + DK - 1) / DK * DK;
