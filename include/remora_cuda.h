@@ -200,7 +200,7 @@ typedef struct {
     double tol;          /* backward-error target (<= 0: 1e-15) */
     int max_iter;        /* CG iterations allowed in total (< 0: 100) */
     int outer;           /* outer panel width, a multiple of 128 (<= 0: 1024) */
-    double shift_factor; /* theta = shift_factor * u_f; < 0: adaptive (u_f, then 8 and 64 u_f
+    double shift_factor; /* theta = shift_factor * u_f; < 0: adaptive (u_f / 4, then 2 and 16 u_f
                             after a breakdown of the low-precision factorisation) */
 } rc_mixed_options;
 typedef struct {

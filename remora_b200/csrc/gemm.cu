@@ -126,6 +126,13 @@ __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1
         : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// Shared-memory tiles are k-rows of DLDA / LDB doubles; the row offset of element (k, c) is
+// c ^ dswz(k): when the global layout is K-major, consecutive lanes store consecutive k
+// rows, and the XOR spreads their 8-byte stores over all banks (without it the row strides
+// 132 and 68 put four lanes on each bank pair). The fragment loads of one 4-deep k step
+// share one XOR value, which only permutes columns inside groups of four.
+__device__ __forceinline__ int dswz(int k) { return (k >> 2) & 3; }
+
 // A_KMAJOR: A(i, k) is contiguous along k (A.cs == 1), else along i (A.rs == 1).
 // B_KMAJOR: B(k, j) is contiguous along k (B.rs == 1), else along j (B.cs == 1).
 template <bool A_KMAJOR, bool B_KMAJOR, int BN>
@@ -139,7 +146,7 @@ __device__ __forceinline__ void dmma_load_tile(double* sA, double* sB, const Vie
         if (A_KMAJOR) { kk = tid % 16; mm = tid / 16 + 16 * r; } else { mm = tid % 128; kk = tid / 128 + 2 * r; }
         const int64_t gi = m0 + mm, gk = k0 + kk;
         const bool ok = gi < m && gk < k;
-        cp_async8(sA + kk * DLDA + mm, ok ? &A(gi, gk) : A.p, ok);
+        cp_async8(sA + kk * DLDA + (mm ^ dswz(kk)), ok ? &A(gi, gk) : A.p, ok);
     }
 #pragma unroll
     for (int r = 0; r < BN / 16; ++r) {
@@ -147,7 +154,7 @@ __device__ __forceinline__ void dmma_load_tile(double* sA, double* sB, const Vie
         if (B_KMAJOR) { kk = tid % 16; nn = tid / 16 + 16 * r; } else { nn = tid % BN; kk = tid / BN + (256 / BN) * r; }
         const int64_t gj = n0 + nn, gk = k0 + kk;
         const bool ok = gj < n && gk < k;
-        cp_async8(sB + kk * LDB + nn, ok ? &B(gk, gj) : B.p, ok);
+        cp_async8(sB + kk * LDB + (nn ^ dswz(kk)), ok ? &B(gk, gj) : B.p, ok);
     }
 }
 
@@ -204,13 +211,14 @@ __global__ void __launch_bounds__(256, 1) gemm_dmma_f64(int64_t m, int64_t n, in
 #pragma unroll
         for (int ks = 0; ks < DK; ks += 4) {
             double af[MI][2], bf[NI];
+            const int sx = dswz(ks);  // == dswz(ks + t) for t < 4
 #pragma unroll
             for (int mi = 0; mi < MI; ++mi) {
-                af[mi][0] = a_s[(ks + t) * DLDA + wm + mi * 16 + g];
-                af[mi][1] = a_s[(ks + t) * DLDA + wm + mi * 16 + g + 8];
+                af[mi][0] = a_s[(ks + t) * DLDA + ((wm + mi * 16 + g) ^ sx)];
+                af[mi][1] = a_s[(ks + t) * DLDA + ((wm + mi * 16 + g + 8) ^ sx)];
             }
 #pragma unroll
-            for (int ni = 0; ni < NI; ++ni) bf[ni] = b_s[(ks + t) * LDB + wn + ni * 8 + g];
+            for (int ni = 0; ni < NI; ++ni) bf[ni] = b_s[(ks + t) * LDB + ((wn + ni * 8 + g) ^ sx)];
 #pragma unroll
             for (int mi = 0; mi < MI; ++mi)
 #pragma unroll

@@ -777,11 +777,13 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     if (o.tol <= 0) o.tol = 1e-15;
     if (o.max_iter < 0) o.max_iter = 100;
     const double uf = prec == RC_PREC_BF16 ? std::ldexp(1.0, -8) : std::ldexp(1.0, -11);
-    // shift_factor < 0: adaptive -- theta = u_f first (measured: a better preconditioner
-    // than no shift at kappa = 1e6, ~100 vs ~180-260 CG steps), then 8 and 64 u_f after a
-    // breakdown of the low-precision factorisation.
+    // shift_factor < 0: adaptive -- theta = u_f / 4 first, then 2 and 16 u_f after a
+    // breakdown of the low-precision factorisation. Measured CG steps at n = 16384 (TF32)
+    // for theta = 0, u_f / 16, u_f / 4, u_f: kappa 1e2: 5, 5, 5, 6; kappa 1e4: 14, 14, 14,
+    // 16; kappa 1e6: 191, 100, 83, 100 -- no shift starves the ill-conditioned case, a
+    // full u_f over-damps the well-conditioned one.
     const bool adaptive = o.shift_factor < 0.0;
-    double theta = adaptive ? uf : o.shift_factor * uf;
+    double theta = adaptive ? 0.25 * uf : o.shift_factor * uf;
 
     size_t bytes = 0;
     mixed_workspace_bytes(n, nrhs, prec, o.outer, &bytes);
@@ -829,7 +831,7 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
             cudaStreamSynchronize(s) != cudaSuccess)
             return RC_ERR_CUDA;
         if (h_info == 0 || !adaptive || attempt == 2) break;
-        theta = (attempt == 0 ? 8.0 : 64.0) * uf;
+        theta = (attempt == 0 ? 2.0 : 16.0) * uf;
     }
     cudaEventRecord(e1, s);
     rc_refine_info info = {};
