@@ -136,6 +136,38 @@ int rc_trsm_f64(int left, int upper, int trans, int unit, size_t m, size_t n, do
 int rc_trsm_f32(int left, int upper, int trans, int unit, size_t m, size_t n, float alpha,
                 const float* A, size_t lda, float* B, size_t ldb, int* d_info, void* stream);
 
+/* y <- alpha * op(A) x + beta * y with A column-major m x n (lda >= m); op(A) = A (trans = 0:
+ * x has n entries, y has m) or A^T (trans = 1: x has m, y has n); incx, incy >= 1 are the
+ * vector strides. Replaces kernels::gemv for hip_tag (include/remora/kernels/hip/
+ * gemv.hpp:45-90, cuBLAS gemv through hip/cublas_backend.hpp:170-213). */
+int rc_gemv_f64(int trans, size_t m, size_t n, double alpha, const double* A, size_t lda, const double* x,
+                size_t incx, double beta, double* y, size_t incy, void* stream);
+int rc_gemv_f32(int trans, size_t m, size_t n, float alpha, const float* A, size_t lda, const float* x,
+                size_t incx, float beta, float* y, size_t incy, void* stream);
+
+/* x <- op(T)^-1 x for the lower (upper = 0) or upper triangle T of the column-major n x n A
+ * (unit: ones assumed on the diagonal), op(T) = T or T^T (trans); x has stride incx.
+ * Replaces kernels::trsv for hip_tag (include/remora/kernels/hip/trsv.hpp:44-90). */
+int rc_trsv_f64(int upper, int trans, int unit, size_t n, const double* A, size_t lda, double* x, size_t incx,
+                void* stream);
+int rc_trsv_f32(int upper, int trans, int unit, size_t n, const float* A, size_t lda, float* x, size_t incx,
+                void* stream);
+
+/* B <- op(T) B (left) or B op(T) (right) for the lower/upper triangle T of the column-major A
+ * (k x k, k = m on the left, n on the right; unit: ones on the diagonal); B column-major
+ * m x n. Replaces kernels::trmm for hip_tag (include/remora/kernels/hip/trmm.hpp:45-106). */
+int rc_trmm_f64(int left, int upper, int trans, int unit, size_t m, size_t n, const double* A, size_t lda,
+                double* B, size_t ldb, void* stream);
+int rc_trmm_f32(int left, int upper, int trans, int unit, size_t m, size_t n, const float* A, size_t lda,
+                float* B, size_t ldb, void* stream);
+
+/* x <- op(T) x for the triangle T of the column-major n x n A; x has stride incx. Replaces
+ * kernels::trmv for hip_tag (include/remora/kernels/hip/trmv.hpp:44-90). */
+int rc_trmv_f64(int upper, int trans, int unit, size_t n, const double* A, size_t lda, double* x, size_t incx,
+                void* stream);
+int rc_trmv_f32(int upper, int trans, int unit, size_t n, const float* A, size_t lda, float* x, size_t incx,
+                void* stream);
+
 /* In-place Cholesky of the lower (A = L L^T) or upper (A = U^T U) triangle of the n x n
  * column-major A; the opposite triangle is never written. d_info (required): set to 0 on
  * success, else to the GLOBAL 1-based index of the first pivot that is not positive

@@ -63,6 +63,12 @@ class Oracle:
                                                     c_void_p, c_ssize_t, c_ssize_t, c_void_p, c_ssize_t, c_ssize_t]
             getattr(L, f"orc_syrk_{t}").argtypes = [c_int, c_size_t, c_size_t, ct, c_void_p, c_ssize_t, c_ssize_t,
                                                     c_void_p, c_ssize_t, c_ssize_t]
+            getattr(L, f"orc_gemv_{t}").argtypes = [c_size_t, c_size_t, ct, c_void_p, c_ssize_t, c_ssize_t, c_void_p,
+                                                   c_ssize_t, c_void_p, c_ssize_t]
+            getattr(L, f"orc_trsv_{t}").argtypes = [c_int, c_int, c_int, c_size_t, c_void_p, c_ssize_t, c_ssize_t,
+                                                   c_void_p, c_ssize_t]
+            getattr(L, f"orc_trmm_{t}").argtypes = [c_int, c_int, c_size_t, c_size_t, c_void_p, c_ssize_t, c_ssize_t,
+                                                   c_void_p, c_ssize_t, c_ssize_t]
             getattr(L, f"orc_trsm_{t}").argtypes = [c_int, c_int, c_int, c_size_t, c_size_t, c_void_p, c_ssize_t,
                                                     c_ssize_t, c_void_p, c_ssize_t, c_ssize_t]
             getattr(L, f"orc_potrf_{t}").argtypes = [c_int, c_size_t, c_void_p, c_ssize_t, c_ssize_t]
@@ -113,6 +119,23 @@ class Oracle:
         t = "f64" if B.dtype == np.float64 else "f32"
         return getattr(self.lib, f"orc_trsm_{t}")(int(left), int(upper), int(unit), B.shape[0], B.shape[1], _p(A),
                                                   *strides(A), _p(B), *strides(B))
+
+    def gemv(self, A, x, y, alpha=1.0):
+        """y += alpha A x; x, y 1-D (any stride)."""
+        t = "f64" if y.dtype == np.float64 else "f32"
+        getattr(self.lib, f"orc_gemv_{t}")(A.shape[0], A.shape[1], alpha, _p(A), *strides(A), _p(x),
+                                           x.strides[0] // x.itemsize, _p(y), y.strides[0] // y.itemsize)
+
+    def trsv(self, A, x, upper=False, unit=False, left=True) -> int:
+        t = "f64" if x.dtype == np.float64 else "f32"
+        return getattr(self.lib, f"orc_trsv_{t}")(int(left), int(upper), int(unit), A.shape[0], _p(A), *strides(A),
+                                                  _p(x), x.strides[0] // x.itemsize)
+
+    def trmm(self, A, B, upper=False, unit=False):
+        """B <- T B (B 2-D; a vector as an n x 1 array gives trmv)."""
+        t = "f64" if B.dtype == np.float64 else "f32"
+        getattr(self.lib, f"orc_trmm_{t}")(int(upper), int(unit), B.shape[0], B.shape[1], _p(A), *strides(A), _p(B),
+                                           *strides(B))
 
     def potrf(self, A, upper=False) -> int:
         t = "f64" if A.dtype == np.float64 else "f32"
@@ -182,6 +205,13 @@ class Reference:
                                                                c_size_t, ct, ct]
             getattr(L, f"ref_generate_uniform_{t}").argtypes = [c_void_p, c_int, c_size_t, c_size_t, c_void_p,
                                                                 c_size_t, ct, ct]
+        for t, ct in (("f64", c_double), ("f32", c_float)):
+            getattr(L, f"ref_gemv_{t}").argtypes = [c_int, c_size_t, c_size_t, ct, c_void_p, c_size_t, c_void_p,
+                                                   c_void_p]
+            getattr(L, f"ref_trsv_{t}").argtypes = [c_int, c_int, c_int, c_int, c_size_t, c_void_p, c_size_t, c_void_p]
+            getattr(L, f"ref_trmv_{t}").argtypes = [c_int, c_int, c_int, c_size_t, c_void_p, c_size_t, c_void_p]
+            getattr(L, f"ref_trmm_{t}").argtypes = [c_int, c_int, c_int, c_int, c_size_t, c_size_t, c_void_p, c_size_t,
+                                                   c_void_p, c_size_t]
         L.ref_cholesky_solve_f64.argtypes = [c_int, c_int, c_size_t, c_size_t, c_void_p, c_size_t, c_void_p,
                                              c_size_t]
 
@@ -221,6 +251,30 @@ class Reference:
         t = "f64" if B.dtype == np.float64 else "f32"
         return getattr(self.lib, f"ref_trsm_{t}")(int(left), int(upper), int(unit), arm, brm, B.shape[0], B.shape[1],
                                                   _p(A), lda, _p(B), ldb)
+
+    def gemv(self, A, x, y, alpha=1.0):
+        """y += alpha A x (kernels::gemv); x, y contiguous 1-D arrays, y updated in place."""
+        arm, lda = self._ld(A)
+        t = "f64" if y.dtype == np.float64 else "f32"
+        getattr(self.lib, f"ref_gemv_{t}")(arm, A.shape[0], A.shape[1], alpha, _p(A), lda, _p(x), _p(y))
+
+    def trsv(self, A, x, upper=False, unit=False, left=True):
+        """x <- A^-1 x (left) or x A^-1 (right) for the named triangle (kernels::trsv)."""
+        arm, lda = self._ld(A)
+        t = "f64" if x.dtype == np.float64 else "f32"
+        getattr(self.lib, f"ref_trsv_{t}")(int(upper), int(unit), int(left), arm, A.shape[0], _p(A), lda, _p(x))
+
+    def trmv(self, A, x, upper=False, unit=False):
+        arm, lda = self._ld(A)
+        t = "f64" if x.dtype == np.float64 else "f32"
+        getattr(self.lib, f"ref_trmv_{t}")(int(upper), int(unit), arm, A.shape[0], _p(A), lda, _p(x))
+
+    def trmm(self, A, B, upper=False, unit=False):
+        arm, lda = self._ld(A)
+        brm, ldb = self._ld(B)
+        t = "f64" if B.dtype == np.float64 else "f32"
+        getattr(self.lib, f"ref_trmm_{t}")(int(upper), int(unit), arm, brm, B.shape[0], B.shape[1], _p(A), lda, _p(B),
+                                          ldb)
 
     def syrk(self, A, C, alpha=1.0, upper=False):
         arm, lda = self._ld(A)

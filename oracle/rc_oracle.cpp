@@ -143,6 +143,35 @@ int trsm(bool left, bool upper, bool unit, size_t m, size_t n, View<const T> A, 
 	return trsm_left(!upper, unit, n, m, A.t(), B.t());
 }
 
+// gemv: kernels/default/gemv.hpp:41-92 -- y += alpha * A x (one dot product per row).
+template<class T>
+void gemv(size_t m, size_t n, T alpha, View<const T> A, const T* x, ptrdiff_t incx, T* y, ptrdiff_t incy) {
+	for (size_t i = 0; i < m; ++i) {
+		T s = 0;
+		for (size_t j = 0; j < n; ++j) s += A(i, j) * x[(ptrdiff_t)j * incx];
+		y[(ptrdiff_t)i * incy] += alpha * s;
+	}
+}
+
+// trmm / trmv: kernels/default/trmm.hpp:40-120, trmv.hpp:40-96 -- B <- T B for the named
+// triangle T of A (ones on the diagonal when unit), evaluated into a copy.
+template<class T>
+void trmm(bool upper, bool unit, size_t m, size_t n, View<const T> A, View<T> B) {
+	std::vector<T> out(m * n);
+	for (size_t c = 0; c < n; ++c)
+		for (size_t i = 0; i < m; ++i) {
+			T s = unit ? B(i, c) : A(i, i) * B(i, c);
+			if (upper) {
+				for (size_t j = i + 1; j < m; ++j) s += A(i, j) * B(j, c);
+			} else {
+				for (size_t j = 0; j < i; ++j) s += A(i, j) * B(j, c);
+			}
+			out[c * m + i] = s;
+		}
+	for (size_t c = 0; c < n; ++c)
+		for (size_t i = 0; i < m; ++i) B(i, c) = out[c * m + i];
+}
+
 // potrf_block (lower, left-looking, double accumulator): kernels/default/potrf.hpp:42-64.
 // Returns the 1-based index inside the block of the first pivot s <= 0.
 template<class T>
@@ -271,6 +300,34 @@ int orc_trsm_f64(int left, int upper, int unit, size_t m, size_t n, const double
 int orc_trsm_f32(int left, int upper, int unit, size_t m, size_t n, const float* A, ptrdiff_t ars, ptrdiff_t acs,
                  float* B, ptrdiff_t brs, ptrdiff_t bcs) {
 	return trsm<float>(left != 0, upper != 0, unit != 0, m, n, {A, ars, acs}, {B, brs, bcs});
+}
+void orc_gemv_f64(size_t m, size_t n, double alpha, const double* A, ptrdiff_t ars, ptrdiff_t acs, const double* x,
+                  ptrdiff_t incx, double* y, ptrdiff_t incy) {
+	gemv<double>(m, n, alpha, {A, ars, acs}, x, incx, y, incy);
+}
+void orc_gemv_f32(size_t m, size_t n, float alpha, const float* A, ptrdiff_t ars, ptrdiff_t acs, const float* x,
+                  ptrdiff_t incx, float* y, ptrdiff_t incy) {
+	gemv<float>(m, n, alpha, {A, ars, acs}, x, incx, y, incy);
+}
+// trsv: kernels/default/trsv.hpp -- the one-column case of trsm (left), or x A = b as
+// A^T x^T = b^T (right).
+int orc_trsv_f64(int left, int upper, int unit, size_t n, const double* A, ptrdiff_t ars, ptrdiff_t acs, double* x,
+                 ptrdiff_t incx) {
+	if (left) return trsm<double>(true, upper != 0, unit != 0, n, 1, {A, ars, acs}, {x, incx, 0});
+	return trsm<double>(true, upper == 0, unit != 0, n, 1, View<const double>{A, ars, acs}.t(), {x, incx, 0});
+}
+int orc_trsv_f32(int left, int upper, int unit, size_t n, const float* A, ptrdiff_t ars, ptrdiff_t acs, float* x,
+                 ptrdiff_t incx) {
+	if (left) return trsm<float>(true, upper != 0, unit != 0, n, 1, {A, ars, acs}, {x, incx, 0});
+	return trsm<float>(true, upper == 0, unit != 0, n, 1, View<const float>{A, ars, acs}.t(), {x, incx, 0});
+}
+void orc_trmm_f64(int upper, int unit, size_t m, size_t n, const double* A, ptrdiff_t ars, ptrdiff_t acs, double* B,
+                  ptrdiff_t brs, ptrdiff_t bcs) {
+	trmm<double>(upper != 0, unit != 0, m, n, {A, ars, acs}, {B, brs, bcs});
+}
+void orc_trmm_f32(int upper, int unit, size_t m, size_t n, const float* A, ptrdiff_t ars, ptrdiff_t acs, float* B,
+                  ptrdiff_t brs, ptrdiff_t bcs) {
+	trmm<float>(upper != 0, unit != 0, m, n, {A, ars, acs}, {B, brs, bcs});
 }
 size_t orc_potrf_f64(int upper, size_t n, double* A, ptrdiff_t rs, ptrdiff_t cs) {
 	return potrf<double>(upper, n, {A, rs, cs});

@@ -62,6 +62,21 @@ int orc_trsm_f64(int left, int upper, int unit, size_t m, size_t n, const double
                  double* B, ptrdiff_t brs, ptrdiff_t bcs);
 int orc_trsm_f32(int left, int upper, int unit, size_t m, size_t n, const float* A, ptrdiff_t ars, ptrdiff_t acs,
                  float* B, ptrdiff_t brs, ptrdiff_t bcs);
+/* y += alpha * A x (A m x n; x, y with strides incx, incy). */
+void orc_gemv_f64(size_t m, size_t n, double alpha, const double* A, ptrdiff_t ars, ptrdiff_t acs, const double* x,
+                  ptrdiff_t incx, double* y, ptrdiff_t incy);
+void orc_gemv_f32(size_t m, size_t n, float alpha, const float* A, ptrdiff_t ars, ptrdiff_t acs, const float* x,
+                  ptrdiff_t incx, float* y, ptrdiff_t incy);
+/* x <- op(A)^-1 x (left) or solves x A = b in place (right); A the named triangle. */
+int orc_trsv_f64(int left, int upper, int unit, size_t n, const double* A, ptrdiff_t ars, ptrdiff_t acs, double* x,
+                 ptrdiff_t incx);
+int orc_trsv_f32(int left, int upper, int unit, size_t n, const float* A, ptrdiff_t ars, ptrdiff_t acs, float* x,
+                 ptrdiff_t incx);
+/* B <- T B for the named triangle T of A (m x m); B is m x n (n = 1: trmv). */
+void orc_trmm_f64(int upper, int unit, size_t m, size_t n, const double* A, ptrdiff_t ars, ptrdiff_t acs, double* B,
+                  ptrdiff_t brs, ptrdiff_t bcs);
+void orc_trmm_f32(int upper, int unit, size_t m, size_t n, const float* A, ptrdiff_t ars, ptrdiff_t acs, float* B,
+                  ptrdiff_t brs, ptrdiff_t bcs);
 /* In-place Cholesky of the lower (upper = 0) or upper triangle; the other triangle is
  * left untouched. Returns 0, or the 1-based GLOBAL index of the first non-positive pivot. */
 size_t orc_potrf_f64(int upper, size_t n, double* A, ptrdiff_t rs, ptrdiff_t cs);

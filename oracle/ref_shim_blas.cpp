@@ -10,6 +10,10 @@
 //   kernels::trsm<Tri,Side>(A,B)      include/remora/kernels/trsm.hpp:55-65
 //   kernels::syrk<Upper>(A,C,alpha)   include/remora/kernels/syrk.hpp:55-67
 //   kernels::gemm(A,B,C,alpha)        include/remora/kernels/gemm.hpp:85-106
+//   kernels::gemv(A,x,y,alpha)        include/remora/kernels/gemv.hpp:56-69
+//   kernels::trsv<Tri,Side>(A,b)      include/remora/kernels/trsv.hpp:56-65
+//   kernels::trmv<Upper,Unit>(A,b)    include/remora/kernels/trmv.hpp:54-65
+//   kernels::trmm<Upper,Unit>(A,B)    include/remora/kernels/trmm.hpp:53-64
 //   cholesky_decomposition + solve    include/remora/decompositions.hpp:70-115
 //   kernels::generate_normal/uniform/discrete (CPU input generator)
 //                                     include/remora/kernels/default/random.hpp:37-122
@@ -139,6 +143,88 @@ void gen_uniform(std::mt19937& rng, std::size_t rows, std::size_t cols, T* A, st
 	view<T, O> a(A, rows, cols, ld);
 	kernels::generate_uniform(a, rng, low, high);
 }
+template<class T, class O>
+void gemv_impl(std::size_t m, std::size_t n, T alpha, T const* A, std::size_t lda, T const* x, T* y) {
+	view<T const, O> a(A, m, n, lda);
+	vector<T> xv(n), yv(m);
+	for (std::size_t j = 0; j != n; ++j) xv(j) = x[j];
+	for (std::size_t i = 0; i != m; ++i) yv(i) = y[i];
+	kernels::gemv(a, xv, yv, alpha);
+	for (std::size_t i = 0; i != m; ++i) y[i] = yv(i);
+}
+
+template<class T, class O, class Tri, class Side>
+void trsv_impl(std::size_t n, T const* A, std::size_t lda, T* x) {
+	view<T const, O> a(A, n, n, lda);
+	vector<T> xv(n);
+	for (std::size_t j = 0; j != n; ++j) xv(j) = x[j];
+	kernels::trsv<Tri, Side>(a, xv);
+	for (std::size_t j = 0; j != n; ++j) x[j] = xv(j);
+}
+
+template<class T, class O, class Tri>
+void trsv_side(int left, std::size_t n, T const* A, std::size_t lda, T* x) {
+	if (left) trsv_impl<T, O, Tri, remora::left>(n, A, lda, x);
+	else trsv_impl<T, O, Tri, remora::right>(n, A, lda, x);
+}
+
+template<class T, class O>
+void trsv_tri(int upper, int unit, int left, std::size_t n, T const* A, std::size_t lda, T* x) {
+	if (upper) {
+		if (unit) trsv_side<T, O, unit_upper>(left, n, A, lda, x);
+		else trsv_side<T, O, remora::upper>(left, n, A, lda, x);
+	} else {
+		if (unit) trsv_side<T, O, unit_lower>(left, n, A, lda, x);
+		else trsv_side<T, O, remora::lower>(left, n, A, lda, x);
+	}
+}
+
+template<class T, class O, bool Upper, bool Unit>
+void trmv_impl(std::size_t n, T const* A, std::size_t lda, T* x) {
+	view<T const, O> a(A, n, n, lda);
+	vector<T> xv(n);
+	for (std::size_t j = 0; j != n; ++j) xv(j) = x[j];
+	kernels::trmv<Upper, Unit>(a, xv);
+	for (std::size_t j = 0; j != n; ++j) x[j] = xv(j);
+}
+
+template<class T, class O>
+void trmv_tri(int upper, int unit, std::size_t n, T const* A, std::size_t lda, T* x) {
+	if (upper) {
+		if (unit) trmv_impl<T, O, true, true>(n, A, lda, x);
+		else trmv_impl<T, O, true, false>(n, A, lda, x);
+	} else {
+		if (unit) trmv_impl<T, O, false, true>(n, A, lda, x);
+		else trmv_impl<T, O, false, false>(n, A, lda, x);
+	}
+}
+
+template<class T, class OA, class OB, bool Upper, bool Unit>
+void trmm_impl(std::size_t m, std::size_t n, T const* A, std::size_t lda, T* B, std::size_t ldb) {
+	view<T const, OA> a(A, m, m, lda);
+	view<T, OB> b(B, m, n, ldb);
+	kernels::trmm<Upper, Unit>(a, b);
+}
+
+template<class T, class OA, class OB>
+void trmm_tri(int upper, int unit, std::size_t m, std::size_t n, T const* A, std::size_t lda, T* B, std::size_t ldb) {
+	if (upper) {
+		if (unit) trmm_impl<T, OA, OB, true, true>(m, n, A, lda, B, ldb);
+		else trmm_impl<T, OA, OB, true, false>(m, n, A, lda, B, ldb);
+	} else {
+		if (unit) trmm_impl<T, OA, OB, false, true>(m, n, A, lda, B, ldb);
+		else trmm_impl<T, OA, OB, false, false>(m, n, A, lda, B, ldb);
+	}
+}
+
+template<class T>
+void trmm_all(int upper, int unit, int a_rm, int b_rm, std::size_t m, std::size_t n, T const* A, std::size_t lda,
+              T* B, std::size_t ldb) {
+	if (a_rm && b_rm) trmm_tri<T, row_major, row_major>(upper, unit, m, n, A, lda, B, ldb);
+	else if (a_rm) trmm_tri<T, row_major, column_major>(upper, unit, m, n, A, lda, B, ldb);
+	else if (b_rm) trmm_tri<T, column_major, row_major>(upper, unit, m, n, A, lda, B, ldb);
+	else trmm_tri<T, column_major, column_major>(upper, unit, m, n, A, lda, B, ldb);
+}
 }  // namespace
 
 extern "C" {
@@ -193,6 +279,44 @@ int ref_cholesky_solve_f64(int a_rm, int b_rm, std::size_t n, std::size_t nrhs,
 	if (a_rm) return chol_solve_impl<row_major, column_major>(n, nrhs, A, lda, B, ldb);
 	if (b_rm) return chol_solve_impl<column_major, row_major>(n, nrhs, A, lda, B, ldb);
 	return chol_solve_impl<column_major, column_major>(n, nrhs, A, lda, B, ldb);
+}
+
+// Matrix-vector kernels; x and y are contiguous.
+void ref_gemv_f64(int a_rm, std::size_t m, std::size_t n, double alpha, double const* A, std::size_t lda,
+                  double const* x, double* y) {
+	if (a_rm) gemv_impl<double, row_major>(m, n, alpha, A, lda, x, y);
+	else gemv_impl<double, column_major>(m, n, alpha, A, lda, x, y);
+}
+void ref_gemv_f32(int a_rm, std::size_t m, std::size_t n, float alpha, float const* A, std::size_t lda,
+                  float const* x, float* y) {
+	if (a_rm) gemv_impl<float, row_major>(m, n, alpha, A, lda, x, y);
+	else gemv_impl<float, column_major>(m, n, alpha, A, lda, x, y);
+}
+void ref_trsv_f64(int upper, int unit, int left, int a_rm, std::size_t n, double const* A, std::size_t lda,
+                  double* x) {
+	if (a_rm) trsv_tri<double, row_major>(upper, unit, left, n, A, lda, x);
+	else trsv_tri<double, column_major>(upper, unit, left, n, A, lda, x);
+}
+void ref_trsv_f32(int upper, int unit, int left, int a_rm, std::size_t n, float const* A, std::size_t lda,
+                  float* x) {
+	if (a_rm) trsv_tri<float, row_major>(upper, unit, left, n, A, lda, x);
+	else trsv_tri<float, column_major>(upper, unit, left, n, A, lda, x);
+}
+void ref_trmv_f64(int upper, int unit, int a_rm, std::size_t n, double const* A, std::size_t lda, double* x) {
+	if (a_rm) trmv_tri<double, row_major>(upper, unit, n, A, lda, x);
+	else trmv_tri<double, column_major>(upper, unit, n, A, lda, x);
+}
+void ref_trmv_f32(int upper, int unit, int a_rm, std::size_t n, float const* A, std::size_t lda, float* x) {
+	if (a_rm) trmv_tri<float, row_major>(upper, unit, n, A, lda, x);
+	else trmv_tri<float, column_major>(upper, unit, n, A, lda, x);
+}
+void ref_trmm_f64(int upper, int unit, int a_rm, int b_rm, std::size_t m, std::size_t n, double const* A,
+                  std::size_t lda, double* B, std::size_t ldb) {
+	trmm_all<double>(upper, unit, a_rm, b_rm, m, n, A, lda, B, ldb);
+}
+void ref_trmm_f32(int upper, int unit, int a_rm, int b_rm, std::size_t m, std::size_t n, float const* A,
+                  std::size_t lda, float* B, std::size_t ldb) {
+	trmm_all<float>(upper, unit, a_rm, b_rm, m, n, A, lda, B, ldb);
 }
 
 // Seeded host generator (std::mt19937), as the reference's CPU tests and benchmarks use.

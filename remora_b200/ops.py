@@ -245,6 +245,55 @@ def potrf_backward(L: torch.Tensor, Lbar: torch.Tensor, Abar: torch.Tensor | Non
     return Abar
 
 
+def _vec(x: torch.Tensor) -> int:
+    if x.dim() != 1:
+        raise ValueError("expected a vector")
+    return max(x.stride(0), 1)
+
+
+def gemv(A: torch.Tensor, x: torch.Tensor, y: torch.Tensor, alpha: float = 1.0, beta: float = 1.0) -> None:
+    """y <- alpha * A @ x + beta * y (beta = 1 is the reference's kernels::gemv)."""
+    sfx = _sfx(A, x, y)
+    ta, lda = layout(A)
+    m, n = A.shape
+    if x.shape[0] != n or y.shape[0] != m:
+        raise ValueError("gemv: shape mismatch")
+    if ta == 0:
+        call(f"rc_gemv_{sfx}", 0, m, n, alpha, _ptr(A), lda, _ptr(x), _vec(x), beta, _ptr(y), _vec(y), _stream())
+    else:  # A^T is column-major n x m
+        call(f"rc_gemv_{sfx}", 1, n, m, alpha, _ptr(A), lda, _ptr(x), _vec(x), beta, _ptr(y), _vec(y), _stream())
+
+
+def trsv(A: torch.Tensor, x: torch.Tensor, upper: bool = False, unit: bool = False, left: bool = True) -> None:
+    """x <- A^-1 x (left) or solves x A = b in place (right), A the named triangle."""
+    sfx = _sfx(A, x)
+    ta, lda = layout(A)
+    up_stored = bool(upper) != bool(ta)
+    trans = ta if left else 1 - ta
+    call(f"rc_trsv_{sfx}", int(up_stored), trans, int(unit), A.shape[0], _ptr(A), lda, _ptr(x), _vec(x), _stream())
+
+
+def trmm(A: torch.Tensor, B: torch.Tensor, upper: bool = False, unit: bool = False) -> None:
+    """B <- T B for the named triangle T of A (the reference's kernels::trmm)."""
+    sfx = _sfx(A, B)
+    ta, lda = layout(A)
+    tb, ldb = layout(B)
+    up_stored = bool(upper) != bool(ta)
+    m, n = B.shape
+    if tb == 0:
+        call(f"rc_trmm_{sfx}", 1, int(up_stored), ta, int(unit), m, n, _ptr(A), lda, _ptr(B), ldb, _stream())
+    else:  # B^T = B^T T^T, column-major n x m
+        call(f"rc_trmm_{sfx}", 0, int(up_stored), 1 - ta, int(unit), n, m, _ptr(A), lda, _ptr(B), ldb, _stream())
+
+
+def trmv(A: torch.Tensor, x: torch.Tensor, upper: bool = False, unit: bool = False) -> None:
+    """x <- T x for the named triangle T of A (the reference's kernels::trmv)."""
+    sfx = _sfx(A, x)
+    ta, lda = layout(A)
+    up_stored = bool(upper) != bool(ta)
+    call(f"rc_trmv_{sfx}", int(up_stored), ta, int(unit), A.shape[0], _ptr(A), lda, _ptr(x), _vec(x), _stream())
+
+
 def trsm_backward(L: torch.Tensor, X: torch.Tensor, Xbar: torch.Tensor, Lbar: torch.Tensor,
                   trans: bool = False) -> torch.Tensor:
     """Reverse mode of X = L^-1 B (trans: X = L^-T B): Xbar becomes Bbar (returned), Lbar

@@ -129,6 +129,41 @@ def syrk_gemm_fixture(ref: oracle.Reference) -> None:
     np.savez_compressed(OUT / "syrk_gemm.npz", **res)
 
 
+def blas2_fixture(ref: oracle.Reference) -> None:
+    # Matrix-vector kernels on the Test/hip_triangular_solve.cpp:104-122 triangle (size 45)
+    # and a formula-built general matrix: gemv (both orientations of A), trsv (left and
+    # right, all triangles), trmv and trmm (all triangles).
+    size, k = 45, 7
+    A = np.ones((size, size), dtype=np.float64)
+    for i in range(size):
+        for j in range(i + 1):
+            A[i, j] = 0.3 * (0.1 / size * i - 0.05 / (i + 1.0) * j) + (10 if i == j else 0)
+    L = np.tril(A)
+    M = np.fromfunction(lambda i, j: 0.01 * (i - 2 * j) + 0.5 * np.sin(i + j), (size, 31))
+    x = np.fromfunction(lambda i: 0.1 * i - 1.0, (size,))
+    x31 = np.fromfunction(lambda i: 0.05 * i + 0.3, (31,))
+    B = np.fromfunction(lambda i, j: (0.1 / size) * i + 0.1 / k * j, (size, k))
+    res = {"L": L, "M": M, "x": x, "x31": x31, "B": B}
+    for order in ("C", "F"):
+        y = np.full(size, 0.25)
+        ref.gemv(np.array(M, order=order), x31, y, alpha=-1.5)
+        res[f"gemv_{order}"] = y
+    for upper in (0, 1):
+        T = L if not upper else L.T.copy()
+        for unit in (0, 1):
+            for left in (1, 0):
+                v = x.copy()
+                ref.trsv(np.array(T, order="C"), v, upper=bool(upper), unit=bool(unit), left=bool(left))
+                res[f"trsv_u{upper}_d{unit}_l{left}"] = v
+            v = x.copy()
+            ref.trmv(np.array(T, order="F"), v, upper=bool(upper), unit=bool(unit))
+            res[f"trmv_u{upper}_d{unit}"] = v
+            X = np.array(B, order="F")
+            ref.trmm(np.array(T, order="C"), X, upper=bool(upper), unit=bool(unit))
+            res[f"trmm_u{upper}_d{unit}"] = X
+    np.savez_compressed(OUT / "blas2.npz", **res)
+
+
 def solve_fixture(ref: oracle.Reference) -> None:
     # The n = 1024 SPD solve recipe at n = 48: G ~ N(0,1) from mt19937(seed) through the
     # reference CPU generator, A = G G^T / n + 1e-2 I (reference gemm), B ~ N(0,1).
@@ -152,6 +187,7 @@ def main() -> None:
     potrf_fixture(ref)
     trsm_fixture(ref)
     syrk_gemm_fixture(ref)
+    blas2_fixture(ref)
     solve_fixture(ref)
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)

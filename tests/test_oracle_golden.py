@@ -108,6 +108,28 @@ def test_syrk_gemm(orc, golden):
     assert oracle.rel_fro(C, g["G"]) <= 1e-14
 
 
+def test_blas2(orc, golden):
+    """gemv / trsv / trmv / trmm of the oracle against the reference's own kernels."""
+    g = golden("blas2")
+    for order in ("C", "F"):
+        y = np.full(45, 0.25)
+        orc.gemv(np.array(g["M"], order=order), g["x31"], y, alpha=-1.5)
+        assert oracle.rel_fro(y[:, None], g[f"gemv_{order}"][:, None]) <= 1e-14
+    for upper in (0, 1):
+        T = g["L"] if not upper else g["L"].T.copy()
+        for unit in (0, 1):
+            for left in (1, 0):
+                v = g["x"].copy()
+                assert orc.trsv(T, v, upper=bool(upper), unit=bool(unit), left=bool(left)) == 0
+                assert oracle.rel_fro(v[:, None], g[f"trsv_u{upper}_d{unit}_l{left}"][:, None]) <= 1e-13
+            v = g["x"].copy()
+            orc.trmm(T, v[:, None], upper=bool(upper), unit=bool(unit))
+            assert oracle.rel_fro(v[:, None], g[f"trmv_u{upper}_d{unit}"][:, None]) <= 1e-14
+            X = np.array(g["B"], order="F")
+            orc.trmm(T, X, upper=bool(upper), unit=bool(unit))
+            assert oracle.rel_fro(X, g[f"trmm_u{upper}_d{unit}"]) <= 1e-14
+
+
 def test_cholesky_solve(orc, golden):
     g = golden("solve")
     X = np.array(g["B"], order="F")
