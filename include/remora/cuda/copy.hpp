@@ -105,7 +105,107 @@ private:
     device* m_queue;
 };
 
+/// Device vector (dense storage, any stride) -> host vector expression: one pitched copy.
+template <class E>
+class vector_transport_to_host : public vector_expression<vector_transport_to_host<E>, cpu_tag> {
+public:
+    typedef typename E::const_closure_type expression_closure_type;
+    typedef typename E::value_type value_type;
+    typedef typename E::size_type size_type;
+    typedef value_type const& const_reference;
+    typedef const_reference reference;
+    typedef vector_transport_to_host const_closure_type;
+    typedef vector_transport_to_host closure_type;
+    typedef unknown_storage storage_type;
+    typedef unknown_storage const_storage_type;
+    typedef blockwise<typename E::evaluation_category::tag> evaluation_category;
+    typedef no_iterator const_iterator;
+    typedef no_iterator iterator;
+
+    explicit vector_transport_to_host(expression_closure_type const& e) : m_expression(e) {}
+    size_type size() const { return m_expression.size(); }
+    typename device_traits<cpu_tag>::queue_type& queue() const { return device_traits<cpu_tag>::default_queue(); }
+
+    template <class VecX>
+    void assign_to(vector_expression<VecX, cpu_tag>& x) const {
+        auto const& ev = eval_expression(m_expression);
+        auto se = ev.raw_storage();
+        auto sx = x().raw_storage();
+        device& dev = ev.queue();
+        if (size())
+            check(rc_memcpy2d(sx.values, sx.stride * sizeof(value_type), se.values, se.stride * sizeof(value_type),
+                              sizeof(value_type), size(), RC_COPY_D2H, dev.stream()),
+                  "rc_memcpy2d");
+        dev.synchronize();
+    }
+    template <class VecX>
+    void plus_assign_to(vector_expression<VecX, cpu_tag>& x) const {
+        remora::vector<value_type> tmp(size());
+        assign_to(tmp);
+        plus_assign(x, tmp);
+    }
+
+private:
+    expression_closure_type m_expression;
+};
+
+/// Host vector expression -> device vector (dense storage, any stride): the values are
+/// evaluated into a contiguous host vector, then one pitched copy.
+template <class E>
+class vector_transport_to_device : public vector_expression<vector_transport_to_device<E>, cuda_tag> {
+public:
+    typedef typename E::const_closure_type expression_closure_type;
+    typedef typename E::value_type value_type;
+    typedef typename E::size_type size_type;
+    typedef value_type const& const_reference;
+    typedef const_reference reference;
+    typedef vector_transport_to_device const_closure_type;
+    typedef vector_transport_to_device closure_type;
+    typedef unknown_storage storage_type;
+    typedef unknown_storage const_storage_type;
+    typedef blockwise<typename E::evaluation_category::tag> evaluation_category;
+    typedef no_iterator const_iterator;
+    typedef no_iterator iterator;
+
+    vector_transport_to_device(expression_closure_type const& e, device& queue) : m_expression(e), m_queue(&queue) {}
+    size_type size() const { return m_expression.size(); }
+    device& queue() const { return *m_queue; }
+
+    template <class VecX>
+    void assign_to(vector_expression<VecX, cuda_tag>& x) const {
+        remora::vector<value_type> host(m_expression);
+        auto sx = x().raw_storage();
+        if (size())
+            check(rc_memcpy2d(sx.values, sx.stride * sizeof(value_type), host.raw_storage().values,
+                              sizeof(value_type), sizeof(value_type), size(), RC_COPY_H2D, m_queue->stream()),
+                  "rc_memcpy2d");
+        m_queue->synchronize();
+    }
+    template <class VecX>
+    void plus_assign_to(vector_expression<VecX, cuda_tag>& x) const;  // not provided: device += host
+
+private:
+    expression_closure_type m_expression;
+    device* m_queue;
+};
+
 }  // namespace cuda
+
+template <class E>
+cuda::vector_transport_to_host<E> copy_to_cpu(vector_expression<E, cuda_tag> const& e) {
+    return cuda::vector_transport_to_host<E>(e());
+}
+
+template <class E>
+cuda::vector_transport_to_device<E> copy_to_device(vector_expression<E, cpu_tag> const& e, cuda_tag,
+                                                   cuda::device& queue = device_traits<cuda_tag>::default_queue()) {
+    return cuda::vector_transport_to_device<E>(e(), queue);
+}
+
+template <class E>
+E const& copy_to_device(vector_expression<E, cuda_tag> const& e, cuda_tag) {
+    return e();
+}
 
 template <class E>
 cuda::matrix_transport_to_host<E> copy_to_cpu(matrix_expression<E, cuda_tag> const& e) {

@@ -192,6 +192,49 @@ private:
     size_type m_size2;
 };
 
+/// \brief A triangle of a strided device matrix (the cuda_tag specialisation of
+/// dense_triangular_proxy, which to_triangular / triangular_prod build,
+/// include/remora/dense.hpp:258-266): a view tagged with the triangle; kernels read it
+/// through to_dense() and the tag.
+template <class T, class Orientation, bool Upper, bool Unit>
+class dense_triangular_proxy<T, Orientation, triangular_tag<Upper, Unit>, cuda_tag>
+    : public matrix_expression<dense_triangular_proxy<T, Orientation, triangular_tag<Upper, Unit>, cuda_tag>, cuda_tag> {
+public:
+    typedef std::size_t size_type;
+    typedef typename std::remove_const<T>::type value_type;
+    typedef value_type result_type;
+    typedef typename std::conditional<Unit, value_type const&, T&>::type reference;
+    typedef value_type const& const_reference;
+    typedef dense_triangular_proxy<value_type const, Orientation, triangular_tag<Upper, Unit>, cuda_tag>
+        const_closure_type;
+    typedef dense_triangular_proxy closure_type;
+    typedef dense_matrix_storage<T, dense_tag> storage_type;
+    typedef dense_matrix_storage<value_type const, dense_tag> const_storage_type;
+    typedef elementwise<dense_tag> evaluation_category;
+    typedef triangular<Orientation, triangular_tag<Upper, Unit>> orientation;
+
+    template <class U>
+    dense_triangular_proxy(dense_triangular_proxy<U, Orientation, triangular_tag<Upper, Unit>, cuda_tag> const& p)
+        : m_storage(p.raw_storage()), m_queue(&p.queue()), m_size1(p.size1()), m_size2(p.size2()) {}
+    dense_triangular_proxy(storage_type const& storage, cuda::device& queue, size_type size1, size_type size2)
+        : m_storage(storage), m_queue(&queue), m_size1(size1), m_size2(size2) {}
+
+    dense_matrix_adaptor<T, Orientation, dense_tag, cuda_tag> to_dense() const {
+        return {m_storage, *m_queue, m_size1, m_size2};
+    }
+    size_type size1() const { return m_size1; }
+    size_type size2() const { return m_size2; }
+    storage_type raw_storage() const { return m_storage; }
+    cuda::device& queue() const { return *m_queue; }
+    typedef no_iterator major_iterator;
+    typedef no_iterator const_major_iterator;
+
+private:
+    storage_type m_storage;
+    cuda::device* m_queue;
+    size_type m_size1, m_size2;
+};
+
 /// \brief Strided device vector view.
 template <class T, class Tag>
 class dense_vector_adaptor<T, Tag, cuda_tag> : public vector_expression<dense_vector_adaptor<T, Tag, cuda_tag>, cuda_tag> {
@@ -219,6 +262,10 @@ public:
     size_type size() const { return m_size; }
     cuda::device& queue() const { return *m_queue; }
     storage_type raw_storage() const { return m_storage; }
+    typename device_traits<cuda_tag>::template vector_element<T> elements() const {
+        return typename device_traits<cuda_tag>::template vector_element<T>(
+            dense_vector_storage<T, dense_tag>(m_storage.values, m_storage.stride));
+    }
     // A strided vector is the 1 x size column-major matrix with leading dimension = stride.
     void clear() {
         if (m_size)
@@ -255,16 +302,49 @@ public:
         : m_storage(size, queue) {
         cuda::detail::fill<T, column_major>(m_storage.get(), 1, 1, size, init, queue);
     }
+    /// From a device expression: a blockwise one (a transport from the host, a
+    /// matrix-vector product, ...) assigns itself; a dense one is copied.
+    template <class E>
+    vector(vector_expression<E, cuda_tag> const& e) : m_storage(e().size(), e().queue()) {
+        assign_from(e(), typename E::evaluation_category());
+    }
+    template <class E>
+    vector& operator=(vector_expression<E, cuda_tag> const& e) {
+        vector tmp(e);
+        m_storage = std::move(tmp.m_storage);
+        return *this;
+    }
+    vector(vector const& v) = default;
+    vector(vector&& v) = default;
+    vector& operator=(vector const& v) = default;
+    vector& operator=(vector&& v) = default;
+
     size_type size() const { return m_storage.size(); }
     cuda::device& queue() const { return m_storage.dev(); }
     const_storage_type raw_storage() const { return {m_storage.get(), 1}; }
     storage_type raw_storage() { return {m_storage.get(), 1}; }
+    typename device_traits<cuda_tag>::template vector_element<T const> elements() const {
+        return typename device_traits<cuda_tag>::template vector_element<T const>(
+            dense_vector_storage<T const, dense_tag>(m_storage.get(), 1));
+    }
     void resize(size_type size) { m_storage.resize(size); }
     void clear() { cuda::detail::fill<T, column_major>(m_storage.get(), 1, 1, size(), T(), queue()); }
     typedef no_iterator iterator;
     typedef no_iterator const_iterator;
 
 private:
+    template <class E, class Tag>
+    void assign_from(E const& e, blockwise<Tag>) {
+        e.assign_to(*this);
+    }
+    template <class E, class Tag>
+    void assign_from(E const& e, elementwise<Tag>) {  // dense device vector: one strided copy
+        auto se = e.raw_storage();
+        if (size())
+            cuda::check(rc_memcpy2d(m_storage.get(), sizeof(T), se.values, se.stride * sizeof(T), sizeof(T), size(),
+                                    RC_COPY_D2D, queue().stream()),
+                        "rc_memcpy2d");
+    }
     cuda::buffer<T> m_storage;
 };
 

@@ -207,6 +207,26 @@ struct device_traits<cuda_tag> {
         T operator()(T) const { return m_v; }
         T m_v;
     };
+    // Functors of the blockwise assignments Remora issues for scalar-scaled operands
+    // (x = alpha e, x += alpha e); the cuda_tag bindings read their scalar.
+    template <class T>
+    struct multiply_assign {
+        typedef T result_type;
+        explicit multiply_assign(T s) : m_s(s) {}
+        T m_s;
+    };
+    template <class T>
+    struct multiply_and_add {
+        typedef T result_type;
+        explicit multiply_and_add(T s) : m_s(s) {}
+        T m_s;
+    };
+    /// Element-functor composition: element functors are never evaluated by this backend
+    /// (its bindings read dense storage), so the composition is an empty placeholder.
+    template <class F, class G>
+    static no_functor make_compose(F const&, G const&) {
+        return no_functor();
+    }
     template <class T>
     struct matrix_element {
         typedef T& result_type;

@@ -31,6 +31,17 @@ template <class M, class E, class EOrientation, class TagE, class TagM>
 void matrix_assign(matrix_expression<M, cuda_tag>& m, matrix_expression<E, cuda_tag> const& e, row_major,
                    EOrientation, TagE, TagM);
 
+// Scalar assignment X = f(X, t) for the functors Remora's blockwise products issue
+// (kernels/matrix_assign.hpp:58-66: X *= alpha after an in-place triangular product).
+template <class F, class M, class Orientation>
+void matrix_assign(matrix_expression<M, cuda_tag>& m, typename M::value_type t, Orientation);
+// Vector assignment v = e for a dense e or alpha * (dense e) (kernels/vector_assign.hpp:
+// 58-64), and v = alpha e / v += alpha e with a scalar functor (:72-78).
+template <class V, class E, class TagV, class TagE>
+void vector_assign(vector_expression<V, cuda_tag>& v, vector_expression<E, cuda_tag> const& e, TagV, TagE);
+template <class V, class E, class F, class TagV, class TagE>
+void vector_assign_functor(vector_expression<V, cuda_tag>& v, vector_expression<E, cuda_tag> const& e, F f, TagV,
+                           TagE);
 // RNG fills, the hip_tag overloads of kernels/hip/random.hpp:261-323.
 template <class M, class Rng>
 void generate_normal(matrix_expression<M, cuda_tag>& m, Rng& rng, typename M::value_type mean,
@@ -65,6 +76,18 @@ void trsm(matrix_expression<MatA, cuda_tag> const& A, matrix_expression<MatB, cu
 // In-place Cholesky (kernels/potrf.hpp:56-62; hip: kernels/hip/potrf.hpp:131-141).
 template <class Triangular, class MatA>
 std::size_t potrf(matrix_container<MatA, cuda_tag>& A);
+// v += alpha * A x (kernels/gemv.hpp:56-69; hip: kernels/hip/gemv.hpp:45-90).
+template <class MatA, class VecX, class VecV>
+void gemv(matrix_expression<MatA, cuda_tag> const& A, vector_expression<VecX, cuda_tag> const& x,
+          vector_expression<VecV, cuda_tag>& v, typename VecV::value_type const& alpha);
+// Triangular solve with one vector (kernels/trsv.hpp:56-65; hip: kernels/hip/trsv.hpp:44-90).
+template <class Triangular, class Side, class MatA, class VecV>
+void trsv(matrix_expression<MatA, cuda_tag> const& A, vector_expression<VecV, cuda_tag>& v);
+// Triangular products b <- A b, B <- A B (kernels/trmv.hpp:54-65, kernels/trmm.hpp:53-64).
+template <bool Upper, bool Unit, class MatA, class VecV>
+void trmv(matrix_expression<MatA, cuda_tag> const& A, vector_expression<VecV, cuda_tag>& v);
+template <bool Upper, bool Unit, class MatA, class MatB>
+void trmm(matrix_expression<MatA, cuda_tag> const& A, matrix_expression<MatB, cuda_tag>& B);
 }  // namespace kernels
 
 }  // namespace remora

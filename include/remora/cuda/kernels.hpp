@@ -42,6 +42,30 @@ struct blas<double> {
     static int potrf(int up, std::size_t n, double* A, std::size_t lda, int* info, void* s) {
         return rc_potrf_f64(up, n, A, lda, info, s);
     }
+    static int gemv(int t, std::size_t m, std::size_t n, double alpha, double const* A, std::size_t lda, double const* x,
+                    std::size_t incx, double beta, double* y, std::size_t incy, void* s) {
+        return rc_gemv_f64(t, m, n, alpha, A, lda, x, incx, beta, y, incy, s);
+    }
+    static int trsv(int up, int t, int unit, std::size_t n, double const* A, std::size_t lda, double* x, std::size_t incx,
+                    void* s) {
+        return rc_trsv_f64(up, t, unit, n, A, lda, x, incx, s);
+    }
+    static int trmv(int up, int t, int unit, std::size_t n, double const* A, std::size_t lda, double* x, std::size_t incx,
+                    void* s) {
+        return rc_trmv_f64(up, t, unit, n, A, lda, x, incx, s);
+    }
+    static int trmm(int left, int up, int t, int unit, std::size_t m, std::size_t n, double const* A, std::size_t lda,
+                    double* B, std::size_t ldb, void* s) {
+        return rc_trmm_f64(left, up, t, unit, m, n, A, lda, B, ldb, s);
+    }
+    static int axpby(std::size_t n, double alpha, double const* x, std::size_t incx, double beta, double* y, std::size_t incy,
+                     void* s) {
+        return rc_axpby_f64(n, alpha, x, incx, beta, y, incy, s);
+    }
+    static int copy2d(int t, std::size_t m, std::size_t n, double alpha, double const* A, std::size_t lda, double* B,
+                      std::size_t ldb, void* s) {
+        return rc_copy2d_f64(t, m, n, alpha, A, lda, B, ldb, s);
+    }
 };
 template <>
 struct blas<float> {
@@ -60,6 +84,30 @@ struct blas<float> {
     }
     static int potrf(int up, std::size_t n, float* A, std::size_t lda, int* info, void* s) {
         return rc_potrf_f32(up, n, A, lda, info, s);
+    }
+    static int gemv(int t, std::size_t m, std::size_t n, float alpha, float const* A, std::size_t lda, float const* x,
+                    std::size_t incx, float beta, float* y, std::size_t incy, void* s) {
+        return rc_gemv_f32(t, m, n, alpha, A, lda, x, incx, beta, y, incy, s);
+    }
+    static int trsv(int up, int t, int unit, std::size_t n, float const* A, std::size_t lda, float* x, std::size_t incx,
+                    void* s) {
+        return rc_trsv_f32(up, t, unit, n, A, lda, x, incx, s);
+    }
+    static int trmv(int up, int t, int unit, std::size_t n, float const* A, std::size_t lda, float* x, std::size_t incx,
+                    void* s) {
+        return rc_trmv_f32(up, t, unit, n, A, lda, x, incx, s);
+    }
+    static int trmm(int left, int up, int t, int unit, std::size_t m, std::size_t n, float const* A, std::size_t lda,
+                    float* B, std::size_t ldb, void* s) {
+        return rc_trmm_f32(left, up, t, unit, m, n, A, lda, B, ldb, s);
+    }
+    static int axpby(std::size_t n, float alpha, float const* x, std::size_t incx, float beta, float* y, std::size_t incy,
+                     void* s) {
+        return rc_axpby_f32(n, alpha, x, incx, beta, y, incy, s);
+    }
+    static int copy2d(int t, std::size_t m, std::size_t n, float alpha, float const* A, std::size_t lda, float* B,
+                      std::size_t ldb, void* s) {
+        return rc_copy2d_f32(t, m, n, alpha, A, lda, B, ldb, s);
     }
 };
 
@@ -169,6 +217,83 @@ std::size_t potrf(matrix_container<MatA, cuda_tag>& A) {
     return (std::size_t)h;  // 0, or the global 1-based index of the failing pivot
 }
 
+// v += alpha * A x (kernels/gemv.hpp:56-69; hip: kernels/hip/gemv.hpp:45-90).
+template <class MatA, class VecX, class VecV>
+void gemv(matrix_expression<MatA, cuda_tag> const& A, vector_expression<VecX, cuda_tag> const& x,
+          vector_expression<VecV, cuda_tag>& v, typename VecV::value_type const& alpha) {
+    REMORA_SIZE_CHECK(A().size1() == v().size());
+    REMORA_SIZE_CHECK(A().size2() == x().size());
+    typedef typename VecV::value_type T;
+    auto const& Ae = eval_expression(A);
+    auto const& xe = eval_expression(x);
+    auto sa = Ae.raw_storage();
+    auto sx = xe.raw_storage();
+    auto sv = v().raw_storage();
+    const int ta = cuda::detail::trans_of<typename std::decay<decltype(Ae)>::type::orientation>();
+    std::size_t m = A().size1(), n = A().size2();
+    if (ta) std::swap(m, n);  // the column-major storage of a row-major A is A^T
+    cuda::check(cuda::detail::blas<T>::gemv(ta, m, n, alpha, sa.values, sa.leading_dimension, sx.values, sx.stride,
+                                            T(1), sv.values, sv.stride, v().queue().stream()),
+                "rc_gemv");
+}
+
+// b <- A^-1 b (left) or the solution of x A = b (right) (kernels/trsv.hpp:56-65; hip:
+// kernels/hip/trsv.hpp:44-90).
+template <class Triangular, class Side, class MatA, class VecV>
+void trsv(matrix_expression<MatA, cuda_tag> const& A, vector_expression<VecV, cuda_tag>& v) {
+    REMORA_SIZE_CHECK(A().size1() == A().size2());
+    REMORA_SIZE_CHECK(A().size2() == v().size());
+    typedef typename VecV::value_type T;
+    auto const& Ae = eval_expression(A);
+    auto sa = Ae.raw_storage();
+    auto sv = v().raw_storage();
+    const int ta = cuda::detail::trans_of<typename std::decay<decltype(Ae)>::type::orientation>();
+    const int up = (Triangular::is_upper ? 1 : 0) ^ ta;  // the triangle as stored
+    const int trans = Side::is_left ? ta : 1 - ta;       // x A = b is A^T x = b
+    cuda::check(cuda::detail::blas<T>::trsv(up, trans, Triangular::is_unit ? 1 : 0, v().size(), sa.values,
+                                            sa.leading_dimension, sv.values, sv.stride, v().queue().stream()),
+                "rc_trsv");
+}
+
+// b <- A b for the named triangle of A (kernels/trmv.hpp:54-65; hip: kernels/hip/trmv.hpp:44-90).
+template <bool Upper, bool Unit, class MatA, class VecV>
+void trmv(matrix_expression<MatA, cuda_tag> const& A, vector_expression<VecV, cuda_tag>& v) {
+    REMORA_SIZE_CHECK(A().size1() == A().size2());
+    REMORA_SIZE_CHECK(A().size2() == v().size());
+    typedef typename VecV::value_type T;
+    auto const& Ae = eval_expression(A);
+    auto sa = Ae.raw_storage();
+    auto sv = v().raw_storage();
+    const int ta = cuda::detail::trans_of<typename std::decay<decltype(Ae)>::type::orientation>();
+    cuda::check(cuda::detail::blas<T>::trmv((Upper ? 1 : 0) ^ ta, ta, Unit ? 1 : 0, v().size(), sa.values,
+                                            sa.leading_dimension, sv.values, sv.stride, v().queue().stream()),
+                "rc_trmv");
+}
+
+// B <- A B for the named triangle of A (kernels/trmm.hpp:53-64; hip: kernels/hip/trmm.hpp:90-106).
+template <bool Upper, bool Unit, class MatA, class MatB>
+void trmm(matrix_expression<MatA, cuda_tag> const& A, matrix_expression<MatB, cuda_tag>& B) {
+    REMORA_SIZE_CHECK(A().size1() == A().size2());
+    REMORA_SIZE_CHECK(A().size2() == B().size1());
+    typedef typename MatB::value_type T;
+    auto const& Ae = eval_expression(A);
+    auto sa = Ae.raw_storage();
+    auto sb = B().raw_storage();
+    const int ta = cuda::detail::trans_of<typename std::decay<decltype(Ae)>::type::orientation>();
+    const int tb = cuda::detail::trans_of<typename MatB::orientation>();
+    const int up = (Upper ? 1 : 0) ^ ta;
+    int left = 1, trans = ta;
+    std::size_t m = B().size1(), n = B().size2();
+    if (tb) {  // B row-major: B^T <- B^T T^T on the right
+        left = 0;
+        trans = 1 - ta;
+        std::swap(m, n);
+    }
+    cuda::check(cuda::detail::blas<T>::trmm(left, up, trans, Unit ? 1 : 0, m, n, sa.values, sa.leading_dimension,
+                                            sb.values, sb.leading_dimension, B().queue().stream()),
+                "rc_trmm");
+}
+
 }  // namespace kernels
 
 namespace cuda {
@@ -209,6 +334,58 @@ void trsm_backward(bool trans, matrix_expression<ML, cuda_tag> const& L, matrix_
 }  // namespace cuda
 
 namespace bindings {
+
+namespace cuda_detail {
+// v <- alpha * e + beta * v for a device vector e with dense storage.
+template <class V, class E>
+void axpby_dense(vector_expression<V, cuda_tag>& v, E const& e, typename V::value_type alpha,
+                 typename V::value_type beta) {
+    typedef typename V::value_type T;
+    auto se = e.raw_storage();
+    auto sv = v().raw_storage();
+    cuda::check(cuda::detail::blas<T>::axpby(v().size(), alpha, se.values, se.stride, beta, sv.values, sv.stride,
+                                             v().queue().stream()),
+                "rc_axpby");
+}
+template <class V, class E>
+void assign_dense(vector_expression<V, cuda_tag>& v, E const& e, typename V::value_type scale) {
+    axpby_dense(v, e, scale, typename V::value_type(0));
+}
+template <class V, class E>
+void assign_dense(vector_expression<V, cuda_tag>& v, vector_scalar_multiply<E> const& e,
+                  typename V::value_type scale) {
+    assign_dense(v, e.expression(), scale * e.scalar());
+}
+}  // namespace cuda_detail
+
+template <class F, class M, class Orientation>
+void matrix_assign(matrix_expression<M, cuda_tag>& m, typename M::value_type t, Orientation) {
+    typedef typename M::value_type T;
+    static_assert(std::is_same<F, typename device_traits<cuda_tag>::template multiply<T>>::value,
+                  "cuda_tag: only X *= t is provided as a scalar assignment");
+    auto sm = m().raw_storage();
+    const int tm = cuda::detail::trans_of<typename M::orientation>();
+    const std::size_t rows = tm ? m().size2() : m().size1(), cols = tm ? m().size1() : m().size2();
+    cuda::check(cuda::detail::blas<T>::copy2d(0, rows, cols, t, sm.values, sm.leading_dimension, sm.values,
+                                              sm.leading_dimension, m().queue().stream()),
+                "rc_copy2d");
+}
+
+template <class V, class E, class TagV, class TagE>
+void vector_assign(vector_expression<V, cuda_tag>& v, vector_expression<E, cuda_tag> const& e, TagV, TagE) {
+    cuda_detail::assign_dense(v, e(), typename V::value_type(1));
+}
+
+template <class V, class E, class F, class TagV, class TagE>
+void vector_assign_functor(vector_expression<V, cuda_tag>& v, vector_expression<E, cuda_tag> const& e, F f, TagV,
+                           TagE) {
+    typedef typename V::value_type T;
+    typedef typename device_traits<cuda_tag>::template multiply_assign<T> Assign;
+    typedef typename device_traits<cuda_tag>::template multiply_and_add<T> AddAssign;
+    static_assert(std::is_same<F, Assign>::value || std::is_same<F, AddAssign>::value,
+                  "cuda_tag: only v = alpha e and v += alpha e are provided as functor assignments");
+    cuda_detail::axpby_dense(v, e(), f.m_s, std::is_same<F, AddAssign>::value ? T(1) : T(0));
+}
 
 template <class M, class E, class EOrientation, class TagE, class TagM>
 void matrix_assign(matrix_expression<M, cuda_tag>& m, matrix_expression<E, cuda_tag> const& e, row_major,

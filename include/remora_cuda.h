@@ -295,6 +295,12 @@ int rc_copy2d_f64(int trans, size_t m, size_t n, double alpha, const double* A, 
 int rc_copy2d_f32(int trans, size_t m, size_t n, float alpha, const float* A, size_t lda,
                   float* B, size_t ldb, void* stream);
 int rc_fill_f64(size_t m, size_t n, double value, double* A, size_t lda, void* stream);
+/* rc_axpby_*: y <- alpha * x + beta * y for vectors of n entries with strides incx, incy (the
+ * dense vector assignments of include/remora/kernels/hip/vector_assign.hpp:55-130; beta = 0
+ * does not read y). */
+int rc_axpby_f64(size_t n, double alpha, const double* x, size_t incx, double beta, double* y, size_t incy,
+                 void* stream);
+int rc_axpby_f32(size_t n, float alpha, const float* x, size_t incx, float beta, float* y, size_t incy, void* stream);
 int rc_fill_f32(size_t m, size_t n, float value, float* A, size_t lda, void* stream);
 
 #ifdef __cplusplus

@@ -80,6 +80,16 @@ __global__ void tri_copy_kernel(int64_t k, View<const T> S, bool upper, bool uni
         }
 }
 
+// y = alpha x + beta y (beta == 0 does not read y).
+template <class T>
+__global__ void axpby_kernel(int64_t n, T alpha, const T* x, int64_t incx, T beta, T* y, int64_t incy) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        T v = alpha * x[i * incx];
+        if (beta != T(0)) v = fma(beta, y[i * incy], v);
+        y[i * incy] = v;
+    }
+}
+
 dim3 sq_grid(int64_t rows, int64_t cols) {
     return dim3(ceil_div(rows, 256) < 256u ? ceil_div(rows, 256) : 256u, cols < 65535 ? (unsigned)cols : 65535u);
 }
@@ -184,6 +194,16 @@ int trmm_abi(int left, int upper, int trans, int unit, size_t m, size_t n, const
 }
 
 template <class T>
+int axpby_abi(size_t n, T alpha, const T* x, size_t incx, T beta, T* y, size_t incy, void* stream) {
+    if (n == 0) return RC_SUCCESS;
+    if (!x || !y || incx == 0 || incy == 0) return RC_ERR_INVALID_ARGUMENT;
+    const unsigned g = rc::ceil_div(n, 256) < 2048u ? rc::ceil_div(n, 256) : 2048u;
+    rc::axpby_kernel<T><<<g, 256, 0, static_cast<cudaStream_t>(stream)>>>((int64_t)n, alpha, x, (int64_t)incx, beta, y,
+                                                                          (int64_t)incy);
+    return rc::check_launch();
+}
+
+template <class T>
 int trmv_abi(int upper, int trans, int unit, size_t n, const T* A, size_t lda, T* x, size_t incx, void* stream) {
     if (n == 0) return RC_SUCCESS;
     if (!A || !x || lda < n || incx == 0) return RC_ERR_INVALID_ARGUMENT;
@@ -226,6 +246,13 @@ int rc_trmv_f64(int upper, int trans, int unit, size_t n, const double* A, size_
 int rc_trmv_f32(int upper, int trans, int unit, size_t n, const float* A, size_t lda, float* x, size_t incx,
                 void* stream) {
     return trmv_abi<float>(upper, trans, unit, n, A, lda, x, incx, stream);
+}
+int rc_axpby_f64(size_t n, double alpha, const double* x, size_t incx, double beta, double* y, size_t incy,
+                 void* stream) {
+    return axpby_abi<double>(n, alpha, x, incx, beta, y, incy, stream);
+}
+int rc_axpby_f32(size_t n, float alpha, const float* x, size_t incx, float beta, float* y, size_t incy, void* stream) {
+    return axpby_abi<float>(n, alpha, x, incx, beta, y, incy, stream);
 }
 
 }  // extern "C"

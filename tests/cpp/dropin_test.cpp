@@ -34,6 +34,14 @@ static void report(char const* what, double err, double tol) {
     if (!ok) ++failures;
 }
 
+// A host vector as a 1 x n matrix (for rel_diff).
+template <class V>
+matrix<double> to_matrix(V const& v, std::size_t, std::size_t n) {
+    matrix<double> m(1, n);
+    for (std::size_t j = 0; j != n; ++j) m(0, j) = v(j);
+    return m;
+}
+
 // Test/hip_cholesky.cpp:13-33
 matrix<double> createSymm(std::size_t n) {
     matrix<double> R(n, n, 0.0);
@@ -189,6 +197,88 @@ int main() {
         matrix<double, column_major, cuda_tag> Bd2 = copy_to_device(B, cuda_tag());
         matrix<double, column_major, cuda_tag> Xd = solve(Ad, Bd2, symm_pos_def(), left());
         report("solve(A, B, symm_pos_def(), left())", rel_diff(matrix<double>(copy_to_cpu(Xd)), X), 1e-13);
+    }
+    // --- matrix-vector products and vector solves (Test/hip_prod.cpp matrix-vector
+    // cases, Test/hip_triangular_prod.cpp:47-115, decompositions.hpp:111-115)
+    {
+        std::size_t rows = 301, cols = 177;
+        std::mt19937 g(9);
+        matrix<double> M(rows, cols);
+        vector<double> x(cols), y0(rows), xt(rows);
+        kernels::generate_uniform(M, g, -1.0, 1.0);
+        kernels::generate_uniform(x, g, -1.0, 1.0);
+        kernels::generate_uniform(y0, g, -1.0, 1.0);
+        kernels::generate_uniform(xt, g, -1.0, 1.0);
+        vector<double, cuda_tag> xd = copy_to_device(x, cuda_tag());
+        vector<double, cuda_tag> yd = copy_to_device(y0, cuda_tag());
+        matrix<double, row_major, cuda_tag> Mr = copy_to_device(M, cuda_tag());
+        matrix<double, column_major, cuda_tag> Mc = copy_to_device(M, cuda_tag());
+        noalias(yd) += -2.0 * prod(Mr, xd);
+        vector<double> yref = y0;
+        noalias(yref) += -2.0 * prod(M, x);
+        vector<double> yh = copy_to_cpu(yd);
+        report("noalias(y) += -2 prod(A, x)  row-major A (gemv)", rel_diff(matrix<double>(to_matrix(yh, 1, rows)),
+                                                                        matrix<double>(to_matrix(yref, 1, rows))), 1e-13);
+        vector<double, cuda_tag> yc = prod(Mc, xd);
+        vector<double> ych = copy_to_cpu(yc);
+        vector<double> yref2 = prod(M, x);
+        report("y = prod(A, x)  column-major A", rel_diff(matrix<double>(to_matrix(ych, 1, rows)),
+                                                          matrix<double>(to_matrix(yref2, 1, rows))), 1e-13);
+        vector<double, cuda_tag> xtd = copy_to_device(xt, cuda_tag());
+        vector<double, cuda_tag> zt = prod(trans(Mc), xtd);
+        vector<double> zth = copy_to_cpu(zt);
+        vector<double> ztref = prod(trans(M), xt);
+        report("z = prod(trans(A), x) (transposed gemv)", rel_diff(matrix<double>(to_matrix(zth, 1, cols)),
+                                                                  matrix<double>(to_matrix(ztref, 1, cols))), 1e-13);
+        // vector Cholesky solve: two triangular solves with one right-hand side
+        std::size_t n = 300;
+        matrix<double> A = createSymm(n);
+        vector<double> b(n);
+        kernels::generate_uniform(b, g, -1.0, 1.0);
+        matrix<double, column_major, cuda_tag> Ad = copy_to_device(A, cuda_tag());
+        vector<double, cuda_tag> bd = copy_to_device(b, cuda_tag());
+        cholesky_decomposition<matrix<double, column_major, cuda_tag>> chol(Ad);
+        chol.solve(bd, left());
+        vector<double> bref = b;
+        cholesky_decomposition<matrix<double>> cchol(A);
+        cchol.solve(bref, left());
+        vector<double> bh = copy_to_cpu(bd);
+        report("cholesky_decomposition::solve(vector) (trsv)", rel_diff(matrix<double>(to_matrix(bh, 1, n)),
+                                                                         matrix<double>(to_matrix(bref, 1, n))), 1e-13);
+        // triangular products (Test/hip_triangular_prod.cpp:84-109)
+        matrix<double> Lm(n, n);
+        kernels::generate_uniform(Lm, g, -1.0, 1.0);
+        vector<double> v(n);
+        kernels::generate_uniform(v, g, -1.0, 1.0);
+        matrix<double, row_major, cuda_tag> Lr = copy_to_device(Lm, cuda_tag());
+        vector<double, cuda_tag> vd = copy_to_device(v, cuda_tag());
+        vector<double, cuda_tag> tv(n);
+        noalias(tv) = triangular_prod<lower>(Lr, vd);
+        vector<double> tvref(n);
+        noalias(tvref) = triangular_prod<lower>(Lm, v);
+        vector<double> tvh = copy_to_cpu(tv);
+        report("triangular_prod<lower>(A, x) (trmv)", rel_diff(matrix<double>(to_matrix(tvh, 1, n)),
+                                                               matrix<double>(to_matrix(tvref, 1, n))), 1e-13);
+        matrix<double> Bm(n, 9);
+        kernels::generate_uniform(Bm, g, -1.0, 1.0);
+        matrix<double, column_major, cuda_tag> Lc = copy_to_device(Lm, cuda_tag());
+        matrix<double, row_major, cuda_tag> Bd = copy_to_device(Bm, cuda_tag());
+        matrix<double, row_major, cuda_tag> TB(n, 9);
+        noalias(TB) = triangular_prod<upper>(Lc, Bd);
+        matrix<double> TBref(n, 9);
+        noalias(TBref) = triangular_prod<upper>(Lm, Bm);
+        report("triangular_prod<upper>(A, B) (trmm)", rel_diff(matrix<double>(copy_to_cpu(TB)), TBref), 1e-13);
+        // vector triangular solve through solve() (Test/hip_triangular_solve.cpp:19-60)
+        matrix<double> T = Lm;
+        for (std::size_t i = 0; i != n; ++i) T(i, i) += double(n);
+        matrix<double, column_major, cuda_tag> Td = copy_to_device(T, cuda_tag());
+        vector<double, cuda_tag> sd = copy_to_device(v, cuda_tag());
+        kernels::trsv<lower, left>(Td, sd);
+        vector<double> sref = v;
+        kernels::trsv<lower, left>(T, sref);
+        vector<double> sh = copy_to_cpu(sd);
+        report("kernels::trsv<lower, left>(A, b)", rel_diff(matrix<double>(to_matrix(sh, 1, n)),
+                                                            matrix<double>(to_matrix(sref, 1, n))), 1e-13);
     }
     // --- normal fill through the expression API (Test/hip_random.cpp:79-121): moments
     {
