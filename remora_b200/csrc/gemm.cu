@@ -93,11 +93,12 @@ __global__ void __launch_bounds__(256) gemm_simt(int64_t m, int64_t n, int64_t k
 }
 
 // ------------------------------------------------------------------------------------
-// FP64 DMMA kernel: 128 x BN tiles (BN = 128 or 64 for skinny right-hand sides), k-step 16,
+// FP64 DMMA kernel: 128 x BN tiles (BN = 128 or 64 for skinny right-hand sides), k-step 16
+// staged through a 4-deep cp.async ring,
 // 8 warps. gridDim.z > 1 splits K: slice z covers [z * kchunk, (z + 1) * kchunk) and
 // writes its partial product (alpha = 1, beta = 0) to Cz + z * zstride; a second kernel
 // then reduces the slices into C.
-constexpr int DM = 128, DK = 16, DSTAGES = 3, DPAD = 4;
+constexpr int DM = 128, DK = 16, DSTAGES = 4, DPAD = 4;
 constexpr int DLDA = DM + DPAD;
 
 template <int BN>
@@ -141,17 +142,17 @@ __device__ __forceinline__ void dmma_load_tile(double* sA, double* sB, const Vie
                                                int64_t m0, int64_t n0, int64_t k0, int tid) {
     constexpr int LDB = DmmaCfg<BN>::LDB;
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
+    for (int r = 0; r < DM * DK / 256; ++r) {
         int mm, kk;
-        if (A_KMAJOR) { kk = tid % 16; mm = tid / 16 + 16 * r; } else { mm = tid % 128; kk = tid / 128 + 2 * r; }
+        if (A_KMAJOR) { kk = tid % DK; mm = tid / DK + (256 / DK) * r; } else { mm = tid % DM; kk = tid / DM + (256 / DM) * r; }
         const int64_t gi = m0 + mm, gk = k0 + kk;
         const bool ok = gi < m && gk < k;
         cp_async8(sA + kk * DLDA + (mm ^ dswz(kk)), ok ? &A(gi, gk) : A.p, ok);
     }
 #pragma unroll
-    for (int r = 0; r < BN / 16; ++r) {
+    for (int r = 0; r < BN * DK / 256; ++r) {
         int nn, kk;
-        if (B_KMAJOR) { kk = tid % 16; nn = tid / 16 + 16 * r; } else { nn = tid % BN; kk = tid / BN + (256 / BN) * r; }
+        if (B_KMAJOR) { kk = tid % DK; nn = tid / DK + (256 / DK) * r; } else { nn = tid % BN; kk = tid / BN + (256 / BN) * r; }
         const int64_t gj = n0 + nn, gk = k0 + kk;
         const bool ok = gj < n && gk < k;
         cp_async8(sB + kk * LDB + (nn ^ dswz(kk)), ok ? &B(gk, gj) : B.p, ok);
