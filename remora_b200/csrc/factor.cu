@@ -86,19 +86,6 @@ __global__ void __launch_bounds__(NB) trtri_blocks(int64_t m, View<const T> L, b
     store_block<T>(S, W + (size_t)blockIdx.x * NB * NB);
 }
 
-// 1 / sqrt(d) for d > 0: a single-precision seed refined by two Newton-Raphson steps for
-// the reciprocal square root, r <- r (3 - d r^2) / 2 (quadratic convergence: ~2^-22 ->
-// ~2^-44 -> rounding level), which is much shorter than the double-precision library
-// call on the factorisation's critical path. Outside the float range: the library call.
-__device__ __forceinline__ double recip_sqrt(double d) {
-    if (!(d > 1e-30 && d < 1e30)) return rsqrt(d);
-    double r = (double)rsqrtf((float)d);
-    const double h = 0.5 * d;
-    r = r * fma(-h * r, r, 1.5);
-    r = r * fma(-h * r, r, 1.5);
-    return r;
-}
-
 // In-CTA blocked factorisation of one NB x NB diagonal block (FP64 in shared memory S,
 // row-major, odd stride SLD so that both row and column walks are bank-conflict free).
 // Besides L (lower triangle of S) it keeps rd[i] = 1 / L(i, i) and builds inv(L) in the
@@ -235,7 +222,7 @@ __global__ void __launch_bounds__(256, 1) potrf_diag(View<T> A, int sz, int64_t 
                     if (bad < 0) bad = j;
                     d = 1.0;
                 }
-                const double r = recip_sqrt(d);
+                const double r = rsqrt(d);
                 const double l = lane == j ? d * r : a[j] * r;  // L(i, j); zero above the diagonal
                 a[j] = l;
                 if (lane == j) rd[c0 + j] = r;
@@ -244,7 +231,8 @@ __global__ void __launch_bounds__(256, 1) potrf_diag(View<T> A, int sz, int64_t 
 #pragma unroll
                 for (int c = 0; c < DB; ++c) {
                     if (c <= j) continue;
-                    if (lane >= c) a[c] = fma(-l, colj[c], a[c]);  // a(i, c) -= L(i, j) L(c, j)
+                    const double t = fma(-l, colj[c], a[c]);  // a(i, c) -= L(i, j) L(c, j), lower part only
+                    a[c] = lane >= c ? t : a[c];
                 }
                 __syncwarp();
             }
