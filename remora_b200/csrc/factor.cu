@@ -231,8 +231,9 @@ __global__ void __launch_bounds__(256, 1) potrf_diag(View<T> A, int sz, int64_t 
 #pragma unroll
                 for (int c = 0; c < DB; ++c) {
                     if (c <= j) continue;
-                    const double t = fma(-l, colj[c], a[c]);  // a(i, c) -= L(i, j) L(c, j), lower part only
-                    a[c] = lane >= c ? t : a[c];
+                    // a(i, c) -= L(i, j) L(c, j); lanes above the diagonal only touch their
+                    // upper-triangle entries, which are neither read nor written back
+                    a[c] = fma(-l, colj[c], a[c]);
                 }
                 __syncwarp();
             }
