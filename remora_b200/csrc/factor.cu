@@ -140,32 +140,45 @@ __device__ void inverse_merge(double* S, double* T, int J0, int t, int phase) {
     for (int r = 0; r < NR; ++r)
 #pragma unroll
         for (int q = 0; q < NQ; ++q) acc[r][q] = 0.0;
+    // The triangular operand is walked in k-blocks matching this thread's row or column
+    // blocks: blocks that are entirely zero are skipped, full blocks need no mask, and only
+    // the diagonal block selects.
+    if (phase == 0) {  // T(i, c) = sum_{k >= c} C(i, k) inv(A)(k, c); columns c = tx + 16 q
+#pragma unroll
+        for (int kb = 0; kb < NQ; ++kb) {
 #pragma unroll 4
-    for (int k = 0; k < H; ++k) {
-        double lr[NR], lc[NQ];
-        if (phase == 0) {  // C(i, k) = L(I0 + i, J0 + k); inv(A)(k, c) = S[(J0 + c) SLD + J0 + k], k >= c
+            for (int kk = 0; kk < 16; ++kk) {
+                const int k = 16 * kb + kk;
+                double lr[NR];
 #pragma unroll
-            for (int r = 0; r < NR; ++r) lr[r] = S[(I0 + ty + RY * r) * SLD + J0 + k];
+                for (int r = 0; r < NR; ++r) lr[r] = S[(I0 + ty + RY * r) * SLD + J0 + k];
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-                const int c = tx + 16 * q;
-                const double v = S[(J0 + c) * SLD + J0 + k];
-                lc[q] = k >= c ? v : 0.0;
+                for (int q = 0; q <= kb; ++q) {
+                    double v = S[(J0 + tx + 16 * q) * SLD + J0 + k];  // inv(A)(k, c)
+                    if (q == kb) v = kk >= tx ? v : 0.0;
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) acc[r][q] = fma(lr[r], v, acc[r][q]);
+                }
             }
-        } else {           // inv(D)(i, k) = S[(I0 + k) SLD + I0 + i], k <= i; T(k, c)
-#pragma unroll
-            for (int r = 0; r < NR; ++r) {
-                const int i = ty + RY * r;
-                const double v = S[(I0 + k) * SLD + I0 + i];
-                lr[r] = k <= i ? v : 0.0;
-            }
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) lc[q] = T[k * 65 + tx + 16 * q];
         }
+    } else {           // X(i, c) = -sum_{k <= i} inv(D)(i, k) T(k, c); rows i = ty + RY r
 #pragma unroll
-        for (int r = 0; r < NR; ++r)
+        for (int kb = 0; kb < NR; ++kb) {
+#pragma unroll 4
+            for (int kk = 0; kk < RY; ++kk) {
+                const int k = RY * kb + kk;
+                double lc[NQ];
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) acc[r][q] = fma(lr[r], lc[q], acc[r][q]);
+                for (int q = 0; q < NQ; ++q) lc[q] = T[k * 65 + tx + 16 * q];
+#pragma unroll
+                for (int r = kb; r < NR; ++r) {
+                    double v = S[(I0 + k) * SLD + I0 + ty + RY * r];  // inv(D)(i, k)
+                    if (r == kb) v = kk <= ty ? v : 0.0;
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) acc[r][q] = fma(v, lc[q], acc[r][q]);
+                }
+            }
+        }
     }
 #pragma unroll
     for (int r = 0; r < NR; ++r)
