@@ -36,6 +36,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "SPD solve TFLOP/s n=32768 mixed+refine vs plain FP64, equal backward error"
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one rc_syrk_tc launch (TF32, CTA
+# pairs) at C = 8192 x 8192, depth 1024: `bench.py --case syrk_tc`.
+SYRK_TC_DRAM_BYTES_8192 = 256.3e6
 
 
 def flops(n: int, nrhs: int) -> float:
@@ -305,9 +308,9 @@ def run_ours(args) -> None:
     achieved = syrk_flops / tk / 1e12
     peak = peaks["bf16_tflops"] if prec else peaks["bf16_tflops"] / 2.0
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu
-    # capture of the TF32 kernel at C = 8192 x 8192, depth 1024 (256.3 MB), scaled to this
-    # shape by the C area it reads and writes ((rows / 8192)^2); not captured for BF16.
-    traffic = None if prec else 256.3e6 * (rows / 8192.0) ** 2
+    # capture of the TF32 kernel at C = 8192 x 8192, depth 1024, scaled to this shape by
+    # the C area it reads and writes ((rows / 8192)^2); not captured for BF16.
+    traffic = None if prec else SYRK_TC_DRAM_BYTES_8192 * (rows / 8192.0) ** 2
     del P, C
     torch.cuda.empty_cache()
 
@@ -340,7 +343,8 @@ def run_ours(args) -> None:
             "fp64_cusolver": {"ms": tcus * 1e3, "tflops": flops(n, nrhs) / tcus / 1e12, "backward_error": cus_bwd},
             "speedup_vs_fp64_plain": t64 / (t / args.steps),
             "speedup_vs_cusolver": tcus / (t / args.steps),
-            "roofline": {"kernel": f"tc_gemm_kernel (lower SYRK {rows}x{rows}x{outer}, {args.precision})",
+            "roofline": {"kernel": f"tc_gemm_pair_kernel (tcgen05 cta_group::2, lower SYRK {rows}x{rows}x{outer}, "
+                                   f"{args.precision})",
                          "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "traffic_source": "ncu DRAM bytes of the 8192 x 8192 x 1024 launch scaled by C area"

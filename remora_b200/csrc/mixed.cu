@@ -627,7 +627,7 @@ struct Mixed {
     // its right (T2, the bulk of the flops), so the latency-bound 128-column steps run in
     // the shadow of the trailing update:
     //   look-ahead: pack(p) -> rec(packed) -> wait(T2(p-1)) -> T1(p) -> chain(p + 1)
-    //   main:       wait(packed) -> T2(p) -> rec(T2(p))
+    //   main:       wait(packed) -> T2(p) -> rec(T2(p))      (T2 on CTA pairs, 256 x 256 tiles)
     // T1(p) and T2(p) write disjoint columns; T1(p) waits for T2(p - 1), whose columns
     // include panel p + 1's. BF16 panels are packed into two alternating buffers.
     int factor(int outer, int* info) {
@@ -673,8 +673,8 @@ struct Mixed {
                 const size_t esz = bf16 ? 2 : 4;
                 const void* op2 = static_cast<const char*>(op) + (size_t)w1 * ldo * esz;
                 RC_TRY(ok(cudaStreamWaitEvent(s, ev_packed, 0)));
-                RC_TRY(gemm_tc_kmajor(bf16, r2, r2, w, -1.f, op2, ldo, op2, ldo, 1.f, Wm.sub(k1 + w1, k1 + w1), kLower,
-                                      0, s, info));
+                RC_TRY(gemm_tc_pair_kmajor(bf16, r2, r2, w, -1.f, op2, ldo, op2, ldo, 1.f, Wm.sub(k1 + w1, k1 + w1),
+                                           kLower, 0, s));
                 RC_TRY(ok(cudaEventRecord(ev_t2, s)));
                 t2_pending = true;
             } else {

@@ -207,6 +207,166 @@ __global__ void __launch_bounds__(TC_THREADS, (FOLD || BN == 256) ? 2 : 1)
     }
 }
 
+// Pair kernel: a cluster of two CTAs computes one 256 x 256 tile with
+// tcgen05.mma.cta_group::2. CTA rank r (0 = the leader) stages rows [128 r, 128 r + 128)
+// of the tile's A rows and of its B rows (K-major) in its own shared memory at the same
+// offsets, and holds the accumulator of its 128 rows (x 256 columns) in its own TMEM.
+// Both CTAs issue their TMA loads against the leader's full barrier (peer bit cleared),
+// whose expected byte count covers both; one thread of the leader issues the MMAs and
+// commits every stage to the empty barriers of both CTAs and the final product to both
+// done barriers. Per SM and k-slice this moves 32 KB for a 128 x 256 x 32 product instead
+// of 48 KB, halving the B traffic of the single-CTA 128 x 256 tile. Two CTAs per SM
+// (3 stages each, 256 TMEM columns each). Every mbarrier wait is bounded; every thread of
+// both CTAs reaches the closing cluster barrier.
+constexpr int PAIR_STAGES = 3;
+constexpr int PAIR_A_BYTES = 128 * KB_BYTES, PAIR_B_BYTES = 128 * KB_BYTES;
+constexpr size_t PAIR_SMEM = (size_t)PAIR_STAGES * (PAIR_A_BYTES + PAIR_B_BYTES) + 1024 + 256;
+
+template <bool BF16>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
+    tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int64_t M,
+                        int64_t N, int64_t K, float alpha, float beta, View<float> C, Mask mask, int64_t off,
+                        int* err, uint64_t limit_ns) {
+    constexpr int KB_ELEMS = KB_BYTES / (BF16 ? 2 : 4);
+    constexpr int MMAS_PER_STAGE = KB_BYTES / 32;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + PAIR_STAGES * PAIR_A_BYTES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + PAIR_STAGES * PAIR_B_BYTES);
+    uint64_t* empty = full + PAIR_STAGES;
+    uint64_t* done = empty + PAIR_STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* stop = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const uint32_t rank = cluster_rank();
+    const int64_t m0 = (int64_t)blockIdx.y * 256, n0 = (int64_t)(blockIdx.x >> 1) * 256;
+    if (outside(mask, off, m0, n0, 256, 256)) return;  // the same decision in both CTAs
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < PAIR_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *stop = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(256u));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    tc_fence_before();
+    cluster_sync_all();  // barriers of both CTAs initialised, TMEM allocated in both
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int KB = (int)((K + KB_ELEMS - 1) / KB_ELEMS);
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int issued = 0;
+            for (int kb = 0; kb < KB; ++kb) {
+                const int s = kb % PAIR_STAGES;
+                const uint32_t ph = (kb / PAIR_STAGES) & 1;
+                if (!mbar_wait_bounded(&empty[s], ph ^ 1, stop, limit_ns)) {
+                    raise_stop(stop, err);
+                    break;
+                }
+                if (rank == 0) mbar_expect_tx(&full[s], 2 * (PAIR_A_BYTES + PAIR_B_BYTES));
+                tma_load_2d_pair(sA + s * PAIR_A_BYTES, &tmA, &full[s], kb * KB_ELEMS, (int)(m0 + 128 * rank));
+                tma_load_2d_pair(sB + s * PAIR_B_BYTES, &tmB, &full[s], kb * KB_ELEMS, (int)(n0 + 128 * rank));
+                ++issued;
+            }
+            (void)issued;
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && rank == 0) {
+            const uint32_t fmt = BF16 ? 1u : 2u;
+            const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(256 >> 3) << 17) |
+                                   ((uint32_t)(256 >> 4) << 24);
+            for (int kb = 0; kb < KB; ++kb) {
+                const int s = kb % PAIR_STAGES;
+                const uint32_t ph = (kb / PAIR_STAGES) & 1;
+                if (!mbar_wait_bounded(&full[s], ph, stop, limit_ns)) {
+                    raise_stop(stop, err);
+                    break;
+                }
+                tc_fence_after();
+                const uint64_t ad = sw128_kmajor_desc(sA + s * PAIR_A_BYTES);
+                const uint64_t bd = sw128_kmajor_desc(sB + s * PAIR_B_BYTES);
+#pragma unroll
+                for (int kk = 0; kk < MMAS_PER_STAGE; ++kk)
+                    umma_pair<BF16>(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
+                umma_commit_pair(&empty[s]);
+            }
+            umma_commit_pair(done);
+        }
+    } else {
+        const int q = warp & 3;  // TMEM lane quadrant this warp may access
+        const bool ok = mbar_wait_bounded(done, 0, stop, limit_ns);
+        if (!ok) raise_stop(stop, err);
+        tc_fence_after();
+        if (__all_sync(0xffffffffu, ok && !*stop)) {
+            const int64_t i = m0 + 128 * rank + 32 * q + lane;
+            const bool row_ok = i < M;
+            const bool vec = C.cs == 1 && (C.rs % 4 == 0) && (reinterpret_cast<uintptr_t>(C.p) % 16 == 0);
+#pragma unroll 1
+            for (int c0 = 0; c0 < 256; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+                if (!row_ok) continue;
+                const int64_t j0 = n0 + c0;
+                if (vec && j0 + 15 < N && keep(mask, off, i, j0 + 15) && keep(mask, off, i, j0)) {
+                    float4* dst = reinterpret_cast<float4*>(C.p + i * C.rs + j0);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        float4 r = make_float4(alpha * v[4 * u], alpha * v[4 * u + 1], alpha * v[4 * u + 2],
+                                               alpha * v[4 * u + 3]);
+                        if (beta != 0.f) {
+                            const float4 c = dst[u];
+                            r.x = fmaf(beta, c.x, r.x); r.y = fmaf(beta, c.y, r.y);
+                            r.z = fmaf(beta, c.z, r.z); r.w = fmaf(beta, c.w, r.w);
+                        }
+                        dst[u] = r;
+                    }
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        const int64_t j = j0 + u;
+                        if (j >= N || !keep(mask, off, i, j)) continue;
+                        float r = alpha * v[u];
+                        if (beta != 0.f) r = fmaf(beta, C(i, j), r);
+                        C(i, j) = r;
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    cluster_sync_all();  // the leader's MMAs read this CTA's shared memory until `done`
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u));
+    }
+}
+
+template <bool BF16>
+int launch_tc_pair(const CUtensorMap& ta, const CUtensorMap& tb, int64_t m, int64_t n, int64_t k, float alpha,
+                   float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s) {
+    if (cudaFuncSetAttribute(tc_gemm_pair_kernel<BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)PAIR_SMEM) != cudaSuccess)
+        return RC_ERR_CUDA;
+    dim3 grid(2 * ceil_div(n, 256), ceil_div(m, 256));
+    if (grid.y > 65535) return RC_ERR_NOT_SUPPORTED;
+    tc_gemm_pair_kernel<BF16><<<grid, TC_THREADS, PAIR_SMEM, s>>>(ta, tb, m, n, k, alpha, beta, C, mask, off,
+                                                                  error_word(), wait_limit_ns());
+    return check_launch();
+}
+
 // Split x into TF32 high part (low 13 mantissa bits cleared) and the FP32 remainder,
 // writing K-major copies: dst row r = [hi(.., k) | hi or lo | ...] per `pattern`.
 // Operand layout in dst (rows x 3K, ld = ldd): segments s = 0, 1, 2 of width K hold
@@ -296,6 +456,19 @@ int gemm_tc_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, cons
     }
     return bn == 256 ? launch_tc<256, false>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort)
                      : launch_tc<128, false>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort);
+}
+
+int gemm_tc_pair_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, const void* A, int64_t lda,
+                        const void* B, int64_t ldb, float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s) {
+    if (m <= 0 || n <= 0) return RC_SUCCESS;
+    const int es = bf16 ? 2 : 4;
+    if (k <= 0 || (reinterpret_cast<uintptr_t>(A) % 16) || (reinterpret_cast<uintptr_t>(B) % 16) || ((lda * es) % 16) ||
+        ((ldb * es) % 16) || m > (int64_t)INT32_MAX || n > (int64_t)INT32_MAX || k > (int64_t)INT32_MAX)
+        return RC_ERR_NOT_SUPPORTED;
+    CUtensorMap ta, tb;
+    if (!make_tmap(&ta, A, bf16, m, k, lda, 128) || !make_tmap(&tb, B, bf16, n, k, ldb, 128)) return RC_ERR_NOT_SUPPORTED;
+    return bf16 ? launch_tc_pair<true>(ta, tb, m, n, k, alpha, beta, C, mask, off, s)
+                : launch_tc_pair<false>(ta, tb, m, n, k, alpha, beta, C, mask, off, s);
 }
 
 int gemm_tc_fold_kmajor(int64_t m, int64_t k, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
@@ -398,9 +571,14 @@ int rc_syrk_tc(int precision, size_t n, size_t k, float alpha, const void* P, si
     if (precision != RC_PREC_TF32 && precision != RC_PREC_BF16) return RC_ERR_INVALID_ARGUMENT;
     if (n == 0) return RC_SUCCESS;
     if (!C || ldc < n || (k > 0 && (!P || ldp < k))) return RC_ERR_INVALID_ARGUMENT;
-    return rc::gemm_tc_kmajor(precision == RC_PREC_BF16, (int64_t)n, (int64_t)n, (int64_t)k, alpha, P, (int64_t)ldp, P,
-                              (int64_t)ldp, beta, rc::View<float>{C, (int64_t)ldc, 1}, rc::kLower, 0,
-                              static_cast<cudaStream_t>(stream));
+    const bool bf16 = precision == RC_PREC_BF16;
+    const rc::View<float> Cv{C, (int64_t)ldc, 1};
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (k > 0 && n >= 256)  // CTA pairs on 256 x 256 tiles
+        return rc::gemm_tc_pair_kmajor(bf16, (int64_t)n, (int64_t)n, (int64_t)k, alpha, P, (int64_t)ldp, P,
+                                       (int64_t)ldp, beta, Cv, rc::kLower, 0, s);
+    return rc::gemm_tc_kmajor(bf16, (int64_t)n, (int64_t)n, (int64_t)k, alpha, P, (int64_t)ldp, P, (int64_t)ldp, beta,
+                              Cv, rc::kLower, 0, s);
 }
 
 int rc_selftest_wait_timeout(uint64_t limit_ns, void* stream) {
