@@ -37,9 +37,10 @@ constexpr int TC_THREADS = 192;
 
 template <int BN, bool FOLD = false>
 struct TcCfg {
-    // The folded skinny update (3 stages) and the 128 x 256 tiles (2 stages) run two CTAs
-    // per SM: a second CTA's main loop overlaps one CTA's pipeline fill and epilogue.
-    static constexpr int STAGES = FOLD ? 3 : (BN == 256 ? 2 : 6);
+    // Every configuration runs two CTAs per SM (~96 KB of rings each): a second CTA's main
+    // loop overlaps one CTA's pipeline fill and epilogue, and the factorisation's
+    // look-ahead kernels fit beside a trailing-update CTA.
+    static constexpr int STAGES = FOLD ? 3 : (BN == 256 ? 2 : 3);
     static constexpr int A_BYTES = 128 * KB_BYTES;
     static constexpr int B_BYTES = BN * KB_BYTES;
     static constexpr size_t SMEM = (size_t)STAGES * (A_BYTES + B_BYTES) + 1024 + 256;
@@ -48,7 +49,7 @@ struct TcCfg {
 // FOLD (BN = 128): the product's columns j and j + 64 are summed into column j of C (an
 // m x 64 result from a 128-row B = [B_hi; B_lo], the two halves of an exact TF32 split).
 template <int BN, bool BF16, bool FOLD = false>
-__global__ void __launch_bounds__(TC_THREADS, (FOLD || BN == 256) ? 2 : 1)
+__global__ void __launch_bounds__(TC_THREADS, 2)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int64_t M,
                    int64_t N, int64_t K, float alpha, float beta, View<float> C, Mask mask, int64_t off,
                    const int* abort, int* err, uint64_t limit_ns) {
