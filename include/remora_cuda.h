@@ -104,6 +104,17 @@ int rc_gemm_f64(int transA, int transB, size_t m, size_t n, size_t k, double alp
 int rc_gemm_f32(int transA, int transB, size_t m, size_t n, size_t k, float alpha,
                 const float* A, size_t lda, const float* B, size_t ldb, float beta,
                 float* C, size_t ldc, void* stream);
+/* FP64 C <- alpha * A * B + beta * C (column-major, no transposes, n <= 64) on the int8
+ * tensor cores: A and B are split into 8 signed 7-bit digits below their row (A) and column
+ * (B) maxima and the 36 digit-pair products of weight above 2^-70 run as exact int8 GEMMs
+ * (Ozaki-Ootomo-Yokota error-free splitting). |error(i, j)| <= ~(2k + 9k) 2^-56
+ * 2^(e_i + f_j) with 2^e_i > max|A(i, :)|, 2^f_j > max|B(:, j)|, plus FP64 rounding of the
+ * sum: FP64-level normwise accuracy. Rows of A / columns of B holding Inf or NaN give NaN.
+ * No reference counterpart (an alternative FP64 product for the skinny products of
+ * iterative refinement). RC_ERR_NOT_SUPPORTED for n > 64. */
+int rc_gemm_f64_sliced(size_t m, size_t n, size_t k, double alpha, const double* A, size_t lda,
+                       const double* B, size_t ldb, double beta, double* C, size_t ldc,
+                       void* stream);
 /* Reduced-precision FP32 GEMMs on the tcgen05 tensor cores with FP32 accumulation:
  * rc_gemm_tf32 truncates the operands to TF32 (10 mantissa bits), rc_gemm_bf16 rounds
  * them to BF16. No reference counterpart (the reference's FP32 gemm is cuBLAS SGEMM);

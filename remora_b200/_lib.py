@@ -54,6 +54,7 @@ SIGNATURES: dict[str, list] = {
     "rc_rng_discrete_i32": [_U4, _Z, _Z, _P, _Z, _I, _I, _I, _P],
     "rc_gemm_f64": [_I, _I, _Z, _Z, _Z, c_double, _P, _Z, _P, _Z, c_double, _P, _Z, _P],
     "rc_gemm_f32": [_I, _I, _Z, _Z, _Z, c_float, _P, _Z, _P, _Z, c_float, _P, _Z, _P],
+    "rc_gemm_f64_sliced": [_Z, _Z, _Z, c_double, _P, _Z, _P, _Z, c_double, _P, _Z, _P],
     "rc_gemm_tf32": [_I, _I, _Z, _Z, _Z, c_float, _P, _Z, _P, _Z, c_float, _P, _Z, _P],
     "rc_gemm_bf16": [_I, _I, _Z, _Z, _Z, c_float, _P, _Z, _P, _Z, c_float, _P, _Z, _P],
     "rc_set_wait_limit_ns": [ctypes.c_uint64],

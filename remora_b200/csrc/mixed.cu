@@ -13,9 +13,13 @@
 //     updates inside the panel and the trailing update run on the tcgen05 tensor cores in
 //     TF32 or BF16 with FP32 accumulation (BF16 operands are packed per panel).
 //  3. Refine in FP64: x0 = M^-1 b with M = S^-1 L L^T S^-1, then preconditioned conjugate
-//     gradients on A (FP64 residuals and matrix products on the DMMA path, FP64 vectors,
-//     the FP32 factor as preconditioner), one independent CG recurrence per right-hand
-//     side, stopped per column when the normwise backward error
+//     gradients on A (FP64 vectors, the FP32 factor as preconditioner), one independent
+//     CG recurrence per right-hand side. The CG products A p and the starting residual
+//     run on the int8 tensor cores on a digit split of A made once, concurrently with the
+//     factorisation (56 bits below each row maximum, every digit product exact); every
+//     residual that decides convergence is an FP64 DMMA product, and a failed check
+//     moves the remaining products to the DMMA path too. Stopped per column when the
+//     normwise backward error
 //         ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
 //     of the TRUE residual is at most tol (CG-based iterative refinement for SPD systems:
 //     Higham & Pranesh 2021; GMRES-IR: Carson & Higham 2017/2018).
@@ -29,6 +33,7 @@
 #include "factor.cuh"
 #include "gemm.cuh"
 #include "mixed.cuh"
+#include "ozaki.cuh"
 #include "tc_gemm.cuh"
 
 namespace cg = cooperative_groups;
@@ -521,6 +526,10 @@ struct Buf {
 
 }  // namespace
 
+// CG products on the int8 digit split of A: up to 64 right-hand sides, n large enough
+// for the split (one pass over A) to pay off.
+static bool sliced_products(int64_t n, int64_t nrhs) { return nrhs <= 64 && n >= 512 && n <= (1 << 21) - 128; }
+
 int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* bytes) {
     const int64_t ldw = (n + 31) / 32 * 32;
     const int64_t nblk = (n + kNB - 1) / kNB;
@@ -545,6 +554,10 @@ int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* 
     add((size_t)((n + BS - 1) / BS) * BS * BS * sizeof(float));      // BS-block inverses
     add((size_t)((n + BS - 1) / BS) * BS * BS / 2 * sizeof(float));  // their scratch
     add((size_t)8 * nrhs * sizeof(double));             // per-column scalars
+    if (sliced_products(n, nrhs)) {
+        add(ozaki_a_bytes(n, n));        // digit split of A
+        add(ozaki_p_bytes(n, n, nrhs));  // digits of one product's right-hand side, partials
+    }
     *bytes = b;
     return RC_SUCCESS;
 }
@@ -562,6 +575,22 @@ cudaStream_t lookahead_stream() {
         if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) return nullptr;
         cudaStream_t st = nullptr;
         if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, hi) != cudaSuccess) return nullptr;
+        streams[dev] = st;
+    }
+    return streams[dev];
+}
+
+// One lowest-priority non-blocking stream per device for work that overlaps the
+// factorisation without delaying it (the digit split of A).
+cudaStream_t background_stream() {
+    static cudaStream_t streams[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!streams[dev]) {
+        int lo = 0, hi = 0;
+        if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) return nullptr;
+        cudaStream_t st = nullptr;
+        if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, lo) != cudaSuccess) return nullptr;
         streams[dev] = st;
     }
     return streams[dev];
@@ -589,6 +618,9 @@ struct Mixed {
     float* Tinv;
     float* tmp;
     double* dev_scalars;  // 8 x nrhs
+    OzakiA oz;            // digit split of A (valid when use_oz)
+    void* oz_p = nullptr; // one sliced product's buffers
+    bool use_oz = false;
     View<const double> Av() const { return {A, 1, lda}; }
     View<float> Wv() const { return {W, ldw, 1}; }
 
@@ -737,9 +769,10 @@ struct Mixed {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
     }
 
-    // Rout = B - A X (FP64, DMMA).
-    int residual(const double* B, int64_t ldb, const double* X, int64_t ldx, double* Rout) {
+    // Rout = B - A X: FP64 DMMA, or (sliced) on the int8 digit split of A.
+    int residual(const double* B, int64_t ldb, const double* X, int64_t ldx, double* Rout, bool sliced = false) {
         RC_TRY(copy2d<double, double>(n, nrhs, 1.0, View<const double>{B, 1, ldb}, colmajor(Rout, n), s));
+        if (sliced) return ozaki_gemm(oz, nrhs, -1.0, X, ldx, 1.0, Rout, n, oz_p, s);
         return gemm<double>(n, nrhs, n, -1.0, Av(), View<const double>{X, 1, ldx}, 1.0, colmajor(Rout, n), kFull, 0,
                             s);
     }
@@ -814,10 +847,39 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     M.Y = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS);
     M.Tinv = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS / 2);
     M.dev_scalars = buf.take<double>((size_t)8 * nrhs);
+    void* oz_a = nullptr;
+    if (sliced_products(n, nrhs)) {
+        oz_a = buf.take<char>(ozaki_a_bytes(n, n));
+        M.oz_p = buf.take<char>(ozaki_p_bytes(n, n, nrhs));
+    }
 
     cudaEvent_t e0, e1, e2;
     cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
     cudaEventRecord(e0, s);
+    // The digit split of A runs on a background stream while A is factored.
+    // Every exit leaves s ordered after the split, so that whoever synchronises s before
+    // reusing or growing the workspace also waits for it.
+    struct SplitEvents {
+        cudaStream_t s;
+        cudaEvent_t fork = nullptr, ready = nullptr;
+        bool recorded = false;
+        ~SplitEvents() {
+            if (recorded) cudaStreamWaitEvent(s, ready, 0);
+            if (fork) cudaEventDestroy(fork);
+            if (ready) cudaEventDestroy(ready);
+        }
+    } split{s};
+    if (oz_a) {
+        cudaStream_t bg = background_stream();
+        if (bg && cudaEventCreateWithFlags(&split.fork, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&split.ready, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventRecord(split.fork, s) == cudaSuccess && cudaStreamWaitEvent(bg, split.fork, 0) == cudaSuccess) {
+            const int st = ozaki_prepare_a(n, n, A, lda, oz_a, &M.oz, bg);
+            split.recorded = cudaEventRecord(split.ready, bg) == cudaSuccess;
+            M.use_oz = st == RC_SUCCESS && split.recorded;
+        }
+        cudaGetLastError();
+    }
     const View<const double> Av = M.Av();
     diag_scale_kernel<<<ceil_div(n, 256) < 1024u ? ceil_div(n, 256) : 1024u, 256, 0, s>>>(n, Av, M.sc);
     RC_TRY(check_launch());
@@ -866,6 +928,8 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     }
     RC_TRY(build_block_inverses(n, M.W, M.ldw, M.Winv, M.Y, M.Tinv, s));
     RC_TRY(M.precond(B, ldb, X, ldx));
+    if (M.use_oz && cudaStreamWaitEvent(s, split.ready, 0) != cudaSuccess) return RC_ERR_CUDA;
+    bool sliced = M.use_oz;  // CG products on the digit split until a convergence check fails
     std::vector<char> done(nrhs, 0);
     int iters = 0, residuals = 0;
     double worst = 0.0;
@@ -874,19 +938,27 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     const int64_t ldm = n;
     while (true) {
         if (restart) {
-            RC_TRY(M.residual(B, ldb, X, ldx, Rm));
-            ++residuals;
-            RC_TRY(M.col_reduce(Rm, ldm, nullptr, 0, 0, normR, M.dev_scalars));
-            RC_TRY(M.col_reduce(X, ldx, nullptr, 0, 0, normX, M.dev_scalars + nrhs));
-            worst = 0.0;
-            for (int64_t j = 0; j < nrhs; ++j) {
-                const double eta = normR[j] / (normA * normX[j] + normB[j]);
-                done[j] = !(eta > o.tol);
-                if (std::isfinite(eta)) worst = std::max(worst, eta);
-                else worst = INFINITY;
-            }
+            // The starting residual may come from the digit split; a residual that ends
+            // the solve (or checks a converged recurrence) is always an FP64 DMMA product.
             bool all = true;
-            for (char d : done) all = all && d;
+            for (int pass = 0; pass < 2; ++pass) {
+                const bool from_split = sliced && iters == 0 && pass == 0;
+                RC_TRY(M.residual(B, ldb, X, ldx, Rm, from_split));
+                ++residuals;
+                RC_TRY(M.col_reduce(Rm, ldm, nullptr, 0, 0, normR, M.dev_scalars));
+                RC_TRY(M.col_reduce(X, ldx, nullptr, 0, 0, normX, M.dev_scalars + nrhs));
+                worst = 0.0;
+                for (int64_t j = 0; j < nrhs; ++j) {
+                    const double eta = normR[j] / (normA * normX[j] + normB[j]);
+                    done[j] = !(eta > o.tol);
+                    if (std::isfinite(eta)) worst = std::max(worst, eta);
+                    else worst = INFINITY;
+                }
+                all = true;
+                for (char d : done) all = all && d;
+                if (!from_split || !(all || iters >= o.max_iter)) break;
+            }
+            if (iters > 0 && !all) sliced = false;
             if (all || iters >= o.max_iter) break;
             // (re)start CG from the true residual: Z = M^-1 R, P = Z, rz = R.Z
             RC_TRY(M.precond_RZ());
@@ -895,8 +967,10 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
             restart = false;
         }
         // Q = A P; alpha = rz / (P.Q) on the active columns.
-        RC_TRY(gemm<double>(n, nrhs, n, 1.0, Av, View<const double>{M.P, 1, ldm}, 0.0, colmajor(M.Q, ldm), kFull, 0,
-                            s));
+        if (sliced) RC_TRY(ozaki_gemm(M.oz, nrhs, 1.0, M.P, ldm, 0.0, M.Q, ldm, M.oz_p, s));
+        else
+            RC_TRY(gemm<double>(n, nrhs, n, 1.0, Av, View<const double>{M.P, 1, ldm}, 0.0, colmajor(M.Q, ldm),
+                                kFull, 0, s));
         RC_TRY(M.col_reduce(M.P, ldm, M.Q, ldm, 1, pq, M.dev_scalars));
         for (int64_t j = 0; j < nrhs; ++j) alpha[j] = (done[j] || pq[j] <= 0.0) ? 0.0 : rz[j] / pq[j];
         RC_TRY(M.upload(alpha, M.dev_scalars + 2 * nrhs));

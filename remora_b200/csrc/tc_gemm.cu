@@ -438,6 +438,8 @@ int launch_tc(const CUtensorMap& ta, const CUtensorMap& tb, int64_t m, int64_t n
 
 }  // namespace
 
+void* tensor_map_encoder() { return reinterpret_cast<void*>(encoder()); }
+
 int gemm_tc_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, const void* A, int64_t lda, const void* B,
                    int64_t ldb, float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s, const int* abort,
                    int bn) {

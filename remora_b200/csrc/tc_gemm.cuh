@@ -24,6 +24,9 @@ int gemm_tc_pair_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha,
 int gemm_tc_fold_kmajor(int64_t m, int64_t k, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
                         float beta, View<float> C, cudaStream_t s, const int* abort = nullptr);
 
+// The driver's cuTensorMapEncodeTiled (a PFN_cuTensorMapEncodeTiled_v12000), or null.
+void* tensor_map_encoder();
+
 // Copy rows x K of X into a K-major buffer (row stride ldd), as FP32 or rounded to BF16.
 int pack_kmajor(int64_t rows, int64_t K, View<const float> X, void* dst, int64_t ldd, bool bf16, cudaStream_t s);
 

@@ -82,6 +82,21 @@ def gemm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, alpha: float = 1.0, 
              _stream())
 
 
+def gemm_sliced(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, alpha: float = 1.0, beta: float = 1.0) -> None:
+    """FP64 C <- alpha * A @ B + beta * C on the int8 tensor cores (digit-split operands),
+    column-major A, B, C and at most 64 columns of B."""
+    m, n = C.shape
+    k = A.shape[1]
+    if A.shape[0] != m or B.shape != (k, n):
+        raise ValueError("gemm_sliced: shape mismatch")
+    ta, lda = layout(A)
+    tb, ldb = layout(B)
+    tc, ldc = layout(C)
+    if ta or tb or tc:
+        raise ValueError("gemm_sliced: column-major operands only")
+    call("rc_gemm_f64_sliced", m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb, beta, _ptr(C), ldc, _stream())
+
+
 def syrk(A: torch.Tensor, C: torch.Tensor, alpha: float = 1.0, upper: bool = False, beta: float = 1.0) -> None:
     """One triangle of C <- alpha * A @ A^T + beta * C; the other triangle is untouched."""
     sfx = _sfx(A, C)
