@@ -15,8 +15,9 @@
 //  3. Refine in FP64: x0 = M^-1 b with M = S^-1 L L^T S^-1, then preconditioned conjugate
 //     gradients on A (FP64 vectors, the FP32 factor as preconditioner), one independent
 //     CG recurrence per right-hand side. The CG products A p and the starting residual
-//     run on the int8 tensor cores on a digit split of A made once, concurrently with the
-//     factorisation (56 bits below each row maximum, every digit product exact); every
+//     run on the int8 tensor cores on a digit split of A made in the same pass over A as
+//     W (rows and columns scaled by 2^e_i >= sqrt(A_ii), which bounds every entry of an
+//     SPD matrix; 56 bits below that bound, every digit product exact); every
 //     residual that decides convergence is an FP64 DMMA product, and a failed check
 //     moves the remaining products to the DMMA path too. Stopped per column when the
 //     normwise backward error
@@ -34,6 +35,7 @@
 #include "gemm.cuh"
 #include "mixed.cuh"
 #include "ozaki.cuh"
+#include "ozaki_digits.cuh"
 #include "tc_gemm.cuh"
 
 namespace cg = cooperative_groups;
@@ -68,6 +70,94 @@ __global__ void __launch_bounds__(256) scale_to_f32_kernel(int64_t n, View<const
     for (int r = ty; r < 32; r += 8) {  // write: consecutive threads walk j (W's unit stride)
         const int64_t i = i0 + r, j = j0 + tx;
         if (i < n && j < n && j <= i) W[i * ldw + j] = tile[tx][r];
+    }
+}
+
+// The first pass over A when the CG products run on its int8 digit split: one read of
+// each 32-row x 128-column tile of column-major A writes
+//  - W = fl32(S A S) + theta I on the tiles that meet the lower triangle (as
+//    scale_to_f32_kernel: the same expression, zeros above the diagonal);
+//  - the 8 digits of A_ij / 2^(e_i + e_j) (rexp from the diagonal) K-major, raising *flag
+//    where an entry is not below its bound;
+//  - per 128-column tile bx, the partial sums of |A_ij| of every row (rsum[bx * Mp + i]).
+__global__ void __launch_bounds__(256) scale_split_kernel(int64_t n, const double* A, int64_t lda, const double* s,
+                                                          double theta, float* W, int64_t ldw, const int* rexp,
+                                                          int* flag, int8_t* Sa, int64_t Mp, int64_t ldk,
+                                                          double* rsum) {
+    extern __shared__ double split_smem[];  // dynamic: above the 48 KB static limit
+    double(*rs)[32] = reinterpret_cast<double(*)[32]>(split_smem);
+    uint32_t(*sm)[32][33] = reinterpret_cast<uint32_t(*)[32][33]>(split_smem + 8 * 32);
+    float(*wt)[129] = reinterpret_cast<float(*)[129]>(reinterpret_cast<uint32_t*>(sm) + kOzSlices * 32 * 33);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t tiles_x = (n + 127) / 128;
+    const int64_t bx = blockIdx.x % tiles_x, i0 = (int64_t)(blockIdx.x / tiles_x) * 32, i = i0 + lane;
+    const int64_t jb = bx * 128, j0 = jb + w * 16;
+    const bool lower = jb <= i0 + 31;
+    const int e = rexp[i];
+    const double si = i < n ? s[i] : 0.0;
+    double x[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) x[c] = (i < n && j0 + c < n) ? A[i + (j0 + c) * lda] : 0.0;
+    double ra = 0.0;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) ra += fabs(x[c]);
+    rs[w][lane] = ra;
+    bool fine = true;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        uint32_t word[kOzSlices] = {};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int64_t j = j0 + 4 * q + c;
+            fine &= digits(x[4 * q + c], e + (j < n ? rexp[j] : 0), word, c);
+        }
+#pragma unroll
+        for (int t = 0; t < kOzSlices; ++t) sm[t][lane][w * 4 + q] = word[t];
+    }
+    if (lower) {
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+            const int64_t j = j0 + c;
+            wt[lane][w * 16 + c] =
+                (i < n && j < n && j <= i) ? (float)(si * x[c] * s[j] + (i == j ? theta : 0.0)) : 0.f;
+        }
+    }
+    if (!fine) atomicOr(flag, 1);
+    __syncthreads();
+    const int r = threadIdx.x >> 3, g = threadIdx.x & 7;
+    const int64_t jw = jb + g * 16;
+    if (jw < ldk) {
+#pragma unroll
+        for (int t = 0; t < kOzSlices; ++t) {
+            const uint4 v = make_uint4(sm[t][r][4 * g], sm[t][r][4 * g + 1], sm[t][r][4 * g + 2], sm[t][r][4 * g + 3]);
+            *reinterpret_cast<uint4*>(Sa + ((int64_t)t * Mp + i0 + r) * ldk + jw) = v;
+        }
+    }
+    if (lower && i0 + r < n) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int64_t j = jw + 4 * q;
+            if (j + 3 < ldw)
+                *reinterpret_cast<float4*>(W + (i0 + r) * ldw + j) =
+                    make_float4(wt[r][16 * g + 4 * q], wt[r][16 * g + 4 * q + 1], wt[r][16 * g + 4 * q + 2],
+                                wt[r][16 * g + 4 * q + 3]);
+        }
+    }
+    if (w == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) t += rs[q][lane];
+        rsum[bx * Mp + i] = t;
+    }
+}
+constexpr size_t kSplitSmem = 8 * 32 * sizeof(double) + kOzSlices * 32 * 33 * 4 + 32 * 129 * 4;
+
+// out[i] = the row sums of |A|: rsum summed over the tile columns in a fixed order.
+__global__ void row_sum_kernel(int64_t n, int64_t tiles_x, const double* rsum, int64_t Mp, double* out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double t = 0.0;
+        for (int64_t b = 0; b < tiles_x; ++b) t += rsum[b * Mp + i];
+        out[i] = t;
     }
 }
 
@@ -557,6 +647,7 @@ int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* 
     if (sliced_products(n, nrhs)) {
         add(ozaki_a_bytes(n, n));        // digit split of A
         add(ozaki_p_bytes(n, n, nrhs));  // digits of one product's right-hand side, partials
+        add((size_t)((n + 127) / 128) * ((n + 127) / 128 * 128) * sizeof(double));  // row-sum partials
     }
     *bytes = b;
     return RC_SUCCESS;
@@ -575,22 +666,6 @@ cudaStream_t lookahead_stream() {
         if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) return nullptr;
         cudaStream_t st = nullptr;
         if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, hi) != cudaSuccess) return nullptr;
-        streams[dev] = st;
-    }
-    return streams[dev];
-}
-
-// One lowest-priority non-blocking stream per device for work that overlaps the
-// factorisation without delaying it (the digit split of A).
-cudaStream_t background_stream() {
-    static cudaStream_t streams[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-    if (!streams[dev]) {
-        int lo = 0, hi = 0;
-        if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) return nullptr;
-        cudaStream_t st = nullptr;
-        if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, lo) != cudaSuccess) return nullptr;
         streams[dev] = st;
     }
     return streams[dev];
@@ -848,46 +923,45 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     M.Tinv = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS / 2);
     M.dev_scalars = buf.take<double>((size_t)8 * nrhs);
     void* oz_a = nullptr;
+    double* rsum = nullptr;
     if (sliced_products(n, nrhs)) {
         oz_a = buf.take<char>(ozaki_a_bytes(n, n));
         M.oz_p = buf.take<char>(ozaki_p_bytes(n, n, nrhs));
+        rsum = buf.take<double>((size_t)((n + 127) / 128) * ((n + 127) / 128 * 128));
     }
 
     cudaEvent_t e0, e1, e2;
     cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
     cudaEventRecord(e0, s);
     // The digit split of A runs on a background stream while A is factored.
-    // Every exit leaves s ordered after the split, so that whoever synchronises s before
-    // reusing or growing the workspace also waits for it.
-    struct SplitEvents {
-        cudaStream_t s;
-        cudaEvent_t fork = nullptr, ready = nullptr;
-        bool recorded = false;
-        ~SplitEvents() {
-            if (recorded) cudaStreamWaitEvent(s, ready, 0);
-            if (fork) cudaEventDestroy(fork);
-            if (ready) cudaEventDestroy(ready);
-        }
-    } split{s};
-    if (oz_a) {
-        cudaStream_t bg = background_stream();
-        if (bg && cudaEventCreateWithFlags(&split.fork, cudaEventDisableTiming) == cudaSuccess &&
-            cudaEventCreateWithFlags(&split.ready, cudaEventDisableTiming) == cudaSuccess &&
-            cudaEventRecord(split.fork, s) == cudaSuccess && cudaStreamWaitEvent(bg, split.fork, 0) == cudaSuccess) {
-            const int st = ozaki_prepare_a(n, n, A, lda, oz_a, &M.oz, bg);
-            split.recorded = cudaEventRecord(split.ready, bg) == cudaSuccess;
-            M.use_oz = st == RC_SUCCESS && split.recorded;
-        }
-        cudaGetLastError();
-    }
     const View<const double> Av = M.Av();
     diag_scale_kernel<<<ceil_div(n, 256) < 1024u ? ceil_div(n, 256) : 1024u, 256, 0, s>>>(n, Av, M.sc);
     RC_TRY(check_launch());
     int h_info = 0;
     for (int attempt = 0;; ++attempt) {
         if (cudaMemsetAsync(d_info, 0, sizeof(int), s) != cudaSuccess) return RC_ERR_CUDA;
-        scale_to_f32_kernel<<<dim3(ceil_div(n, 32), ceil_div(n, 32)), 256, 0, s>>>(n, Av, M.sc, theta, M.W, M.ldw);
-        RC_TRY(check_launch());
+        // The first attempt reads A once for W, the digit split and the row sums of |A|. (A
+        // split run on another stream beside the factorisation slows its latency-bound
+        // diagonal chain by more than the split costs.)
+        if (attempt == 0 && oz_a && ozaki_layout_a(n, n, oz_a, true, &M.oz) == RC_SUCCESS) {
+            RC_TRY(ozaki_diag_exponents(M.oz, A, lda, s));
+            if (cudaFuncSetAttribute(scale_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kSplitSmem) != cudaSuccess)
+                return RC_ERR_CUDA;
+            const int64_t tiles = ((n + 127) / 128) * (M.oz.Mp / 32);
+            scale_split_kernel<<<(unsigned)tiles, 256, kSplitSmem, s>>>(n, A, lda, M.sc, theta, M.W, M.ldw, M.oz.rexp,
+                                                                        M.oz.flag, M.oz.slices, M.oz.Mp, M.oz.ldk,
+                                                                        rsum);
+            RC_TRY(check_launch());
+            row_sum_kernel<<<ceil_div(n, 256) < 1024u ? ceil_div(n, 256) : 1024u, 256, 0, s>>>(
+                n, (n + 127) / 128, rsum, M.oz.Mp, M.colsum);
+            RC_TRY(check_launch());
+            M.use_oz = true;
+        } else {
+            scale_to_f32_kernel<<<dim3(ceil_div(n, 32), ceil_div(n, 32)), 256, 0, s>>>(n, Av, M.sc, theta, M.W,
+                                                                                      M.ldw);
+            RC_TRY(check_launch());
+        }
         RC_TRY(M.factor(o.outer, d_info));
         if (cudaMemcpyAsync(&h_info, d_info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess)
@@ -903,9 +977,12 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
         return RC_SUCCESS;  // d_info reports the failing pivot of the low-precision factor
     }
 
-    // ||A||_inf, ||b||_inf per column.
-    col_abs_sum_kernel<<<(unsigned)(n < 4096 ? n : 4096), 256, 0, s>>>(n, Av, M.colsum);
-    RC_TRY(check_launch());
+    // ||A||_inf (the row sums of |A| from the first pass when the split ran, else the
+    // column sums of the symmetric A), ||b||_inf per column.
+    if (!M.use_oz) {
+        col_abs_sum_kernel<<<(unsigned)(n < 4096 ? n : 4096), 256, 0, s>>>(n, Av, M.colsum);
+        RC_TRY(check_launch());
+    }
     std::vector<double> tmpv;
     {
         // max over the n column sums: reuse the column reduction with c = 1 on an n x 1 block
@@ -913,9 +990,12 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
         RC_TRY(check_launch());
     }
     double normA = 0.0;
+    int split_flag = 0;
     if (cudaMemcpyAsync(&normA, M.dev_scalars, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        (M.use_oz && cudaMemcpyAsync(&split_flag, M.oz.flag, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
         cudaStreamSynchronize(s) != cudaSuccess)
         return RC_ERR_CUDA;
+    if (split_flag) M.use_oz = false;  // the diagonal did not bound A: FP64 DMMA products
     std::vector<double> normB, normX, normR, rz, pq, alpha(nrhs), beta(nrhs);
     RC_TRY(M.col_reduce(B, ldb, nullptr, 0, 0, normB, M.dev_scalars));
 
@@ -928,7 +1008,6 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     }
     RC_TRY(build_block_inverses(n, M.W, M.ldw, M.Winv, M.Y, M.Tinv, s));
     RC_TRY(M.precond(B, ldb, X, ldx));
-    if (M.use_oz && cudaStreamWaitEvent(s, split.ready, 0) != cudaSuccess) return RC_ERR_CUDA;
     bool sliced = M.use_oz;  // CG products on the digit split until a convergence check fails
     std::vector<char> done(nrhs, 0);
     int iters = 0, residuals = 0;

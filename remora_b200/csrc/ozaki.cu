@@ -31,6 +31,7 @@
 
 #include "gemm.cuh"
 #include "ozaki.cuh"
+#include "ozaki_digits.cuh"
 #include "tc_common.cuh"
 #include "tc_gemm.cuh"
 
@@ -43,7 +44,7 @@ constexpr int OZ_THREADS = 192;
 constexpr int A_STAGES = 5;
 constexpr int A_TILE = 128 * 128;  // one 128-row x 128-byte slice tile
 constexpr int KC_MAX = 16384;      // S * 127 * 127 * KC_MAX < 2^31
-constexpr int kBadExp = INT_MIN;
+constexpr int kBadExp = kOzBadExp;
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 int64_t round_up(int64_t x, int64_t q) { return (x + q - 1) / q * q; }
@@ -72,32 +73,19 @@ void oz_split(int64_t Mp, int64_t k, int* z_out, int64_t* kc_out) {
     *kc_out = best_kc;
 }
 
-// Exponent e with |x| < 2^e for every x of a row or column whose largest |x| has these
-// bits (0 for an all-zero row; kBadExp when the largest is Inf or NaN).
-__device__ __forceinline__ int scale_exp(unsigned long long bits) {
-    if (bits == 0) return 0;
-    if (bits >= 0x7FF0000000000000ull) return kBadExp;
-    const int ex = (int)(bits >> 52);
-    if (ex == 0) return (63 - __clzll((long long)bits)) - 1073;  // subnormal maximum
-    return ex - 1022;
-}
-
-// The 8 signed base-128 digits of x / 2^e (|x| < 2^e), truncated: V = floor(|x| 2^(56-e))
-// read 7 bits at a time, with x's sign.
-__device__ __forceinline__ void digits(double x, int e, uint32_t (&word)[S], int byte) {
-    const unsigned long long b = (unsigned long long)__double_as_longlong(x);
-    const int ex = (int)((b >> 52) & 0x7FF);
-    const unsigned long long frac = b & 0xFFFFFFFFFFFFFull;
-    const unsigned long long M = ex ? (frac | (1ull << 52)) : frac;
-    const int sh = (ex ? ex : 1) - 1075 + 56 - e;
-    unsigned long long V = 0;
-    if (sh >= 0) V = M << (sh < 63 ? sh : 63);
-    else if (sh > -64) V = M >> (-sh);
-    const bool neg = (b >> 63) != 0;
-#pragma unroll
-    for (int t = 0; t < S; ++t) {
-        const int d = (int)((V >> (49 - 7 * t)) & 127);
-        word[t] |= (uint32_t)(uint8_t)(int8_t)(neg ? -d : d) << (8 * byte);
+// Symmetric scaling from the diagonal (SPD A): 2^e_i >= sqrt(A_ii), so that
+// |A_ij| <= sqrt(A_ii A_jj) < 2^(e_i + e_j). flag is set for a diagonal entry that is not
+// positive and finite.
+__global__ void diag_exp_kernel(int64_t n, const double* A, int64_t lda, int64_t Mp, int* rexp, int* flag) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < Mp; i += (int64_t)gridDim.x * blockDim.x) {
+        int e = 0;
+        if (i < n) {
+            const double d = A[i + i * lda];
+            const int E = scale_exp((unsigned long long)__double_as_longlong(d));  // d < 2^E
+            if (!(d > 0.0) || E == kBadExp) atomicOr(flag, 1);
+            else e = (E + 1) >> 1;  // ceil(E / 2)
+        }
+        rexp[i] = e;
     }
 }
 
@@ -153,15 +141,16 @@ __global__ void __launch_bounds__(256) slice_a_kernel(int64_t m, int64_t k, cons
 
 // One block per column c < nr of P (k x nrhs): its scale exponent, then its digits,
 // K-major: row (t * nr + c) of Ps holds digit t + 1 of column c. Columns c >= nrhs are 0.
+// With pre (the diagonal scaling of A), the digits are those of 2^pre[j] P(j, c).
 __global__ void __launch_bounds__(256) slice_p_kernel(int64_t k, int64_t nrhs, const double* P, int64_t ldp, int nr,
-                                                      int* cexp, int8_t* Ps, int64_t ldk) {
+                                                      const int* pre, int* cexp, int8_t* Ps, int64_t ldk) {
     __shared__ unsigned long long red[8];
     const int c = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     unsigned long long mx = 0;
     if (c < nrhs)
         for (int64_t j = threadIdx.x; j < k; j += 256) {
-            const unsigned long long b =
-                (unsigned long long)__double_as_longlong(P[j + c * ldp]) & 0x7FFFFFFFFFFFFFFFull;
+            const double x = pre ? ldexp(P[j + c * ldp], pre[j]) : P[j + c * ldp];
+            const unsigned long long b = (unsigned long long)__double_as_longlong(x) & 0x7FFFFFFFFFFFFFFFull;
             mx = b > mx ? b : mx;
         }
 #pragma unroll
@@ -182,7 +171,8 @@ __global__ void __launch_bounds__(256) slice_p_kernel(int64_t k, int64_t nrhs, c
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int64_t j = j0 + q;
-            digits((live && j < k) ? P[j + c * ldp] : 0.0, e, word, q);
+            const double x = (live && j < k) ? (pre ? ldexp(P[j + c * ldp], pre[j]) : P[j + c * ldp]) : 0.0;
+            digits(x, e, word, q);
         }
 #pragma unroll
         for (int t = 0; t < S; ++t) *reinterpret_cast<uint32_t*>(Ps + ((int64_t)t * nr + c) * ldk + j0) = word[t];
@@ -381,7 +371,7 @@ bool make_u8_tmap(CUtensorMap* tm, const void* base, int64_t rows, int64_t kdim,
 
 size_t ozaki_a_bytes(int64_t m, int64_t k) {
     const int64_t Mp = round_up(m, 128), ldk = round_up(k, 16);
-    return align256((size_t)S * Mp * ldk) + align256((size_t)Mp * 8) + align256((size_t)Mp * 4);
+    return align256((size_t)S * Mp * ldk) + align256((size_t)Mp * 8) + align256((size_t)Mp * 4) + 256;
 }
 
 size_t ozaki_p_bytes(int64_t m, int64_t k, int64_t nrhs) {
@@ -393,8 +383,8 @@ size_t ozaki_p_bytes(int64_t m, int64_t k, int64_t nrhs) {
     return align256((size_t)S * nr * ldk) + align256((size_t)z * nr * Mp * 8) + align256(64 * 4);
 }
 
-int ozaki_prepare_a(int64_t m, int64_t k, const double* A, int64_t lda, void* ws, OzakiA* out, cudaStream_t s) {
-    if (m <= 0 || k <= 0 || !out) return RC_ERR_INVALID_ARGUMENT;
+int ozaki_layout_a(int64_t m, int64_t k, void* ws, bool diagonal, OzakiA* out) {
+    if (m <= 0 || k <= 0 || !out || (diagonal && m != k)) return RC_ERR_INVALID_ARGUMENT;
     OzakiA a;
     a.m = m;
     a.k = k;
@@ -407,8 +397,28 @@ int ozaki_prepare_a(int64_t m, int64_t k, const double* A, int64_t lda, void* ws
     a.rowbits = reinterpret_cast<unsigned long long*>(p);
     p += align256((size_t)a.Mp * 8);
     a.rexp = reinterpret_cast<int*>(p);
+    p += align256((size_t)a.Mp * 4);
+    a.flag = reinterpret_cast<int*>(p);
+    a.diagonal = diagonal;
     if (!make_u8_tmap(&a.tmap, a.slices, S * a.Mp, k, a.ldk, 128)) return RC_ERR_NOT_SUPPORTED;
-    if (cudaMemsetAsync(a.rowbits, 0, (size_t)a.Mp * 8, s) != cudaSuccess) return RC_ERR_CUDA;
+    *out = a;
+    return RC_SUCCESS;
+}
+
+int ozaki_diag_exponents(const OzakiA& a, const double* A, int64_t lda, cudaStream_t s) {
+    if (!a.diagonal) return RC_ERR_INVALID_ARGUMENT;
+    if (cudaMemsetAsync(a.flag, 0, sizeof(int), s) != cudaSuccess) return RC_ERR_CUDA;
+    diag_exp_kernel<<<ceil_div(a.Mp, 256) < 1024u ? ceil_div(a.Mp, 256) : 1024u, 256, 0, s>>>(a.m, A, lda, a.Mp,
+                                                                                               a.rexp, a.flag);
+    return check_launch();
+}
+
+int ozaki_prepare_a(int64_t m, int64_t k, const double* A, int64_t lda, void* ws, OzakiA* out, cudaStream_t s) {
+    OzakiA a;
+    RC_TRY(ozaki_layout_a(m, k, ws, false, &a));
+    if (cudaMemsetAsync(a.flag, 0, sizeof(int), s) != cudaSuccess ||
+        cudaMemsetAsync(a.rowbits, 0, (size_t)a.Mp * 8, s) != cudaSuccess)
+        return RC_ERR_CUDA;
     row_absmax_kernel<<<dim3(ceil_div(k, 512), ceil_div(m, 256)), 256, 0, s>>>(m, k, A, lda, a.rowbits);
     RC_TRY(check_launch());
     slice_a_kernel<<<dim3(ceil_div(k, 128), (unsigned)(a.Mp / 32)), 256, 0, s>>>(m, k, A, lda, a.rowbits, a.rexp,
@@ -435,7 +445,7 @@ int ozaki_gemm(const OzakiA& a, int64_t nrhs, double alpha, const double* P, int
 
     CUtensorMap tmB;
     if (!make_u8_tmap(&tmB, Ps, S * nr, a.k, a.ldk, S * nr < 256 ? S * nr : 256)) return RC_ERR_NOT_SUPPORTED;
-    slice_p_kernel<<<nr, 256, 0, s>>>(a.k, nrhs, P, ldp, nr, cexp, Ps, a.ldk);
+    slice_p_kernel<<<nr, 256, 0, s>>>(a.k, nrhs, P, ldp, nr, a.diagonal ? a.rexp : nullptr, cexp, Ps, a.ldk);
     RC_TRY(check_launch());
 
     const size_t smem = 1024 + (size_t)A_STAGES * A_TILE + 2 * (size_t)S * nr * 128 + 256;
