@@ -405,6 +405,13 @@ def run_case(args) -> None:
         B = torch.randn((args.nrhs, args.n), device=dev, dtype=torch.float64).t()
         for _ in range(reps):
             ops.spd_solve_mixed(A, B, args.precision, tol=1e-15, max_iter=args.max_iter)
+    elif args.case == "sliced":  # FP64 product on the int8 digit split, 8192 x 8192 times 8192 x 64
+        n = 8192
+        A = torch.randn((n, n), device=dev, dtype=torch.float64).t()
+        P = torch.randn((64, n), device=dev, dtype=torch.float64).t()
+        C = torch.zeros((64, n), device=dev, dtype=torch.float64).t()
+        for _ in range(reps):
+            ops.gemm_sliced(A, P, C, 1.0, 0.0)
     elif args.case == "batched":  # 4096 uneven RBF systems, n ~ U{16..512}
         import numpy as np
         rs = np.random.default_rng(1)
@@ -438,7 +445,7 @@ def main() -> None:
     ap.add_argument("--ref-n", type=int, default=4096, help="CPU reference sample size")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--case", choices=["syrk_tc", "dgemm", "potrf", "rng", "mixed", "batched"],
+    ap.add_argument("--case", choices=["syrk_tc", "dgemm", "potrf", "rng", "mixed", "batched", "sliced"],
                     help="run one small kernel case (for ncu captures) instead of the benchmark")
     args = ap.parse_args()
     if args.case:

@@ -74,52 +74,71 @@ __global__ void __launch_bounds__(256) scale_to_f32_kernel(int64_t n, View<const
 }
 
 // The first pass over A when the CG products run on its int8 digit split: one read of
-// each 32-row x 128-column tile of column-major A writes
+// each 64-row x 128-column tile of column-major A (512 threads; a warp reads 64 rows of a
+// column, 16 bytes per lane when A allows) writes
 //  - W = fl32(S A S) + theta I on the tiles that meet the lower triangle (as
 //    scale_to_f32_kernel: the same expression, zeros above the diagonal);
 //  - the 8 digits of A_ij / 2^(e_i + e_j) (rexp from the diagonal) K-major, raising *flag
 //    where an entry is not below its bound;
 //  - per 128-column tile bx, the partial sums of |A_ij| of every row (rsum[bx * Mp + i]).
-__global__ void __launch_bounds__(256) scale_split_kernel(int64_t n, const double* A, int64_t lda, const double* s,
-                                                          double theta, float* W, int64_t ldw, const int* rexp,
-                                                          int* flag, int8_t* Sa, int64_t Mp, int64_t ldk,
-                                                          double* rsum) {
+constexpr int kSplitRows = 64, kSplitThreads = 512;
+__global__ void __launch_bounds__(kSplitThreads, 2) scale_split_kernel(int64_t n, const double* A, int64_t lda,
+                                                                    const double* s, double theta, float* W,
+                                                                    int64_t ldw, const int* rexp, int* flag,
+                                                                    int8_t* Sa, int64_t Mp, int64_t ldk,
+                                                                    double* rsum) {
     extern __shared__ double split_smem[];  // dynamic: above the 48 KB static limit
-    double(*rs)[32] = reinterpret_cast<double(*)[32]>(split_smem);
-    uint32_t(*sm)[32][33] = reinterpret_cast<uint32_t(*)[32][33]>(split_smem + 8 * 32);
-    float(*wt)[129] = reinterpret_cast<float(*)[129]>(reinterpret_cast<uint32_t*>(sm) + kOzSlices * 32 * 33);
+    double(*rs)[kSplitRows] = reinterpret_cast<double(*)[kSplitRows]>(split_smem);
+    uint32_t(*sm)[kSplitRows][33] = reinterpret_cast<uint32_t(*)[kSplitRows][33]>(split_smem + 16 * kSplitRows);
+    float(*wt)[129] = reinterpret_cast<float(*)[129]>(reinterpret_cast<uint32_t*>(sm) + kOzSlices * kSplitRows * 33);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t tiles_x = (n + 127) / 128;
-    const int64_t bx = blockIdx.x % tiles_x, i0 = (int64_t)(blockIdx.x / tiles_x) * 32, i = i0 + lane;
-    const int64_t jb = bx * 128, j0 = jb + w * 16;
-    const bool lower = jb <= i0 + 31;
-    const int e = rexp[i];
-    const double si = i < n ? s[i] : 0.0;
-    double x[16];
+    const int64_t bx = blockIdx.x % tiles_x, i0 = (int64_t)(blockIdx.x / tiles_x) * kSplitRows;
+    const int64_t jb = bx * 128, j0 = jb + w * 8;
+    const bool lower = jb <= i0 + kSplitRows - 1;
+    const bool vec = (lda % 2 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0);
+    double x[2][8];  // rows i0 + 2 lane + h, columns j0 + c
 #pragma unroll
-    for (int c = 0; c < 16; ++c) x[c] = (i < n && j0 + c < n) ? A[i + (j0 + c) * lda] : 0.0;
-    double ra = 0.0;
+    for (int c = 0; c < 8; ++c) {
+        const int64_t j = j0 + c, ia = i0 + 2 * lane;
+        if (vec && j < n && ia + 1 < n) {
+            const double2 v = *reinterpret_cast<const double2*>(A + ia + j * lda);
+            x[0][c] = v.x;
+            x[1][c] = v.y;
+        } else {
+            x[0][c] = (j < n && ia < n) ? A[ia + j * lda] : 0.0;
+            x[1][c] = (j < n && ia + 1 < n) ? A[ia + 1 + j * lda] : 0.0;
+        }
+    }
+    int ej[8];
 #pragma unroll
-    for (int c = 0; c < 16; ++c) ra += fabs(x[c]);
-    rs[w][lane] = ra;
+    for (int c = 0; c < 8; ++c) ej[c] = j0 + c < n ? rexp[j0 + c] : 0;
     bool fine = true;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        uint32_t word[kOzSlices] = {};
+    for (int h = 0; h < 2; ++h) {
+        const int row = 2 * lane + h;
+        const int64_t i = i0 + row;
+        const int e = rexp[i];
+        double ra = 0.0;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int64_t j = j0 + 4 * q + c;
-            fine &= digits(x[4 * q + c], e + (j < n ? rexp[j] : 0), word, c);
+        for (int c = 0; c < 8; ++c) ra += fabs(x[h][c]);
+        rs[w][row] = ra;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            uint32_t word[kOzSlices] = {};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) fine &= digits(x[h][4 * q + c], e + ej[4 * q + c], word, c);
+#pragma unroll
+            for (int t = 0; t < kOzSlices; ++t) sm[t][row][w * 2 + q] = word[t];
         }
+        if (lower) {
+            const double si = i < n ? s[i] : 0.0;
 #pragma unroll
-        for (int t = 0; t < kOzSlices; ++t) sm[t][lane][w * 4 + q] = word[t];
-    }
-    if (lower) {
-#pragma unroll
-        for (int c = 0; c < 16; ++c) {
-            const int64_t j = j0 + c;
-            wt[lane][w * 16 + c] =
-                (i < n && j < n && j <= i) ? (float)(si * x[c] * s[j] + (i == j ? theta : 0.0)) : 0.f;
+            for (int c = 0; c < 8; ++c) {
+                const int64_t j = j0 + c;
+                wt[row][w * 8 + c] =
+                    (i < n && j < n && j <= i) ? (float)(si * x[h][c] * s[j] + (i == j ? theta : 0.0)) : 0.f;
+            }
         }
     }
     if (!fine) atomicOr(flag, 1);
@@ -143,14 +162,15 @@ __global__ void __launch_bounds__(256) scale_split_kernel(int64_t n, const doubl
                                 wt[r][16 * g + 4 * q + 3]);
         }
     }
-    if (w == 0) {
+    if (threadIdx.x < kSplitRows) {
         double t = 0.0;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) t += rs[q][lane];
-        rsum[bx * Mp + i] = t;
+        for (int q = 0; q < 16; ++q) t += rs[q][threadIdx.x];
+        rsum[bx * Mp + i0 + threadIdx.x] = t;
     }
 }
-constexpr size_t kSplitSmem = 8 * 32 * sizeof(double) + kOzSlices * 32 * 33 * 4 + 32 * 129 * 4;
+constexpr size_t kSplitSmem =
+    16 * kSplitRows * sizeof(double) + kOzSlices * kSplitRows * 33 * 4 + kSplitRows * 129 * 4;
 
 // out[i] = the row sums of |A|: rsum summed over the tile columns in a fixed order.
 __global__ void row_sum_kernel(int64_t n, int64_t tiles_x, const double* rsum, int64_t Mp, double* out) {
@@ -948,8 +968,8 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
             if (cudaFuncSetAttribute(scale_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)kSplitSmem) != cudaSuccess)
                 return RC_ERR_CUDA;
-            const int64_t tiles = ((n + 127) / 128) * (M.oz.Mp / 32);
-            scale_split_kernel<<<(unsigned)tiles, 256, kSplitSmem, s>>>(n, A, lda, M.sc, theta, M.W, M.ldw, M.oz.rexp,
+            const int64_t tiles = ((n + 127) / 128) * (M.oz.Mp / kSplitRows);
+            scale_split_kernel<<<(unsigned)tiles, kSplitThreads, kSplitSmem, s>>>(n, A, lda, M.sc, theta, M.W, M.ldw, M.oz.rexp,
                                                                         M.oz.flag, M.oz.slices, M.oz.Mp, M.oz.ldk,
                                                                         rsum);
             RC_TRY(check_launch());

@@ -23,7 +23,7 @@
 // t at slices + (t * Mp + i) * ldk), in the 128B-swizzled tiles the TMA moves; the digits
 // of P are rebuilt per product, K-major as well (row (u, c) of slice u, column c).
 // Per CTA: warp 0 streams, per 128-wide K block, the 8 x 128-row slices of A through a
-// 5-deep ring and the 8 x nr rows of P's digits through a 2-deep ring; warp 1 issues the
+// 6-deep ring and the 8 x nr rows of P's digits through a 2-deep ring; warp 1 issues the
 // MMAs; warps 2..5 combine the 8 integer accumulators of each row into one FP64 partial.
 // Every mbarrier wait is bounded.
 #include <climits>
@@ -41,7 +41,7 @@ namespace {
 using namespace tc;
 constexpr int S = kOzSlices;
 constexpr int OZ_THREADS = 192;
-constexpr int A_STAGES = 5;
+constexpr int A_STAGES = 6;  // 6 x 16 KB + 2 x 64 KB of P digits: the 227 KB limit
 constexpr int A_TILE = 128 * 128;  // one 128-row x 128-byte slice tile
 constexpr int KC_MAX = 16384;      // S * 127 * 127 * KC_MAX < 2^31
 constexpr int kBadExp = kOzBadExp;
