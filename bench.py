@@ -176,6 +176,14 @@ def max_over_ranks(value: float, device=None) -> float:
     return float(t.item())
 
 
+_T0 = time.perf_counter()
+
+
+def phase(name: str) -> None:
+    """Progress of the default run on stderr (the JSON result line is the only stdout)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f} s] {name}", file=sys.stderr, flush=True)
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -191,6 +199,7 @@ def run_ours(args) -> None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
     lib = _lib.lib()
     n, nrhs = args.n, args.nrhs
+    phase("test matrix")
     A = make_spd(n, args.kappa, seed=1234 + rank, device=dev)
     gB = torch.Generator(device=dev).manual_seed(99 + rank)
     B = torch.randn((nrhs, n), generator=gB, device=dev, dtype=torch.float64).t()  # column-major
@@ -206,9 +215,11 @@ def run_ours(args) -> None:
             dist.barrier()
         torch.cuda.synchronize()
 
+    phase("warm-up")
     for _ in range(args.warmup):
         info, status = step()
     barrier()
+    phase("timed steps")
     launches0 = lib.rc_launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -225,6 +236,7 @@ def run_ours(args) -> None:
     status_ok = all(s == 0 for _, s in infos)
     last = infos[-1][0]
 
+    phase("FP64 comparators")
     # Plain FP64 solve (this library) and the cuSOLVER comparator, same inputs.
     X64 = B.clone()
     torch.cuda.synchronize()
@@ -250,6 +262,7 @@ def run_ours(args) -> None:
     # D2H of X, every step.
     e2e = None
     if not args.no_e2e:
+        phase("end to end from pinned host buffers")
         Ah = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
         Ah.copy_(A)
         Bh = B.cpu().pin_memory()
@@ -277,6 +290,7 @@ def run_ours(args) -> None:
     else:
         del A
 
+    phase("roofline kernel")
     # Roofline: the dominant kernel, the tcgen05 trailing update (lower SYRK C -= P P^T)
     # at the largest trailing shape of the factorisation, timed alone with CUDA events.
     outer = 1024
@@ -316,6 +330,7 @@ def run_ours(args) -> None:
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        phase("CPU reference sample")
         try:
             r = cpu_reference(args.ref_n, nrhs, steps=1, warmup=0)
             cpu = {"value": r["value"], "unit": "TFLOP/s", "cores": 1, "kind": "reference",
