@@ -73,6 +73,9 @@ class Oracle:
                                                     c_ssize_t, c_void_p, c_ssize_t, c_ssize_t]
             getattr(L, f"orc_potrf_{t}").argtypes = [c_int, c_size_t, c_void_p, c_ssize_t, c_ssize_t]
             getattr(L, f"orc_potrf_{t}").restype = c_size_t
+            for f in ("getrf", "pstrf"):
+                getattr(L, f"orc_{f}_{t}").argtypes = [c_size_t, c_void_p, c_ssize_t, c_ssize_t, c_void_p]
+                getattr(L, f"orc_{f}_{t}").restype = c_size_t
         L.orc_cholesky_solve_f64.argtypes = [c_size_t, c_size_t, c_void_p, c_ssize_t, c_ssize_t, c_void_p, c_ssize_t,
                                              c_ssize_t]
         L.orc_cholesky_solve_f64.restype = c_size_t
@@ -141,6 +144,20 @@ class Oracle:
         t = "f64" if A.dtype == np.float64 else "f32"
         return getattr(self.lib, f"orc_potrf_{t}")(int(upper), A.shape[0], _p(A), *strides(A))
 
+    def getrf(self, A) -> tuple[int, np.ndarray]:
+        """LU with partial pivoting in place; returns (status, piv)."""
+        t = "f64" if A.dtype == np.float64 else "f32"
+        piv = np.zeros(A.shape[0], dtype=np.int32)
+        st = getattr(self.lib, f"orc_getrf_{t}")(A.shape[0], _p(A), *strides(A), _p(piv))
+        return st, piv
+
+    def pstrf(self, A) -> tuple[int, np.ndarray]:
+        """Pivoted Cholesky (lower) in place; returns (rank, piv)."""
+        t = "f64" if A.dtype == np.float64 else "f32"
+        piv = np.zeros(A.shape[0], dtype=np.int32)
+        rank = getattr(self.lib, f"orc_pstrf_{t}")(A.shape[0], _p(A), *strides(A), _p(piv))
+        return rank, piv
+
     def cholesky_solve(self, A, B) -> int:
         return self.lib.orc_cholesky_solve_f64(A.shape[0], B.shape[1], _p(A), *strides(A), _p(B), *strides(B))
 
@@ -195,6 +212,10 @@ class Reference:
         for t, ct in (("f64", c_double), ("f32", c_float)):
             getattr(L, f"ref_potrf_{t}").argtypes = [c_int, c_int, c_size_t, c_void_p, c_size_t]
             getattr(L, f"ref_potrf_{t}").restype = c_size_t
+            getattr(L, f"ref_getrf_{t}").argtypes = [c_int, c_size_t, c_void_p, c_size_t, c_void_p]
+            getattr(L, f"ref_getrf_{t}").restype = ctypes.c_long
+            getattr(L, f"ref_pstrf_{t}").argtypes = [c_int, c_size_t, c_void_p, c_size_t, c_void_p]
+            getattr(L, f"ref_pstrf_{t}").restype = c_size_t
             getattr(L, f"ref_trsm_{t}").argtypes = [c_int, c_int, c_int, c_int, c_int, c_size_t, c_size_t, c_void_p,
                                                     c_size_t, c_void_p, c_size_t]
             getattr(L, f"ref_syrk_{t}").argtypes = [c_int, c_int, c_int, c_size_t, c_size_t, ct, c_void_p, c_size_t,
@@ -239,6 +260,20 @@ class Reference:
         out = _U4()
         self.lib.ref_hip_discrete4(_U4(*key), _U4(*ctr), N, out)
         return list(out)
+
+    def getrf(self, A: np.ndarray) -> tuple[int, np.ndarray]:
+        """The reference's kernels::getrf in place; (0 or -1 for its exception, piv)."""
+        rm, ld = self._ld(A)
+        t = "f64" if A.dtype == np.float64 else "f32"
+        piv = np.zeros(A.shape[0], dtype=np.int32)
+        return getattr(self.lib, f"ref_getrf_{t}")(rm, A.shape[0], _p(A), ld, _p(piv)), piv
+
+    def pstrf(self, A: np.ndarray) -> tuple[int, np.ndarray]:
+        """The reference's kernels::pstrf<lower> in place; (rank, piv)."""
+        rm, ld = self._ld(A)
+        t = "f64" if A.dtype == np.float64 else "f32"
+        piv = np.zeros(A.shape[0], dtype=np.int32)
+        return getattr(self.lib, f"ref_pstrf_{t}")(rm, A.shape[0], _p(A), ld, _p(piv)), piv
 
     def potrf(self, A: np.ndarray, upper=False) -> int:
         rm, ld = self._ld(A)

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstring>
 #include <random>
+#include <limits>
 #include <vector>
 
 namespace {
@@ -218,6 +219,127 @@ size_t potrf(int upper, size_t n, View<T> A) {
 	return potrf_rec<T>(n, upper ? A.t() : A, 0);
 }
 
+// ---------------------------------------------------------------------------------------
+// LU with partial pivoting and pivoted Cholesky.
+
+// Row swaps r <-> piv[r] (r = 0, 1, ...) on rows x cols of A; piv relative to A's first row.
+template<class T>
+void swap_rows_seq(size_t count, const int* piv, size_t cols, View<T> A) {
+	for (size_t r = 0; r < count; ++r) {
+		const size_t q = (size_t)piv[r];
+		if (q == r) continue;
+		for (size_t c = 0; c < cols; ++c) std::swap(A(r, c), A(q, c));
+	}
+}
+
+// getrf_block (column-major order): kernels/default/getrf.hpp:41-79 -- per column j the
+// pivot is the first row of largest |A(i, j)| (a later row replaces it only when strictly
+// larger), rows j and pivot are swapped across the panel's columns, the column below the
+// diagonal is divided by the pivot (in double) and the rank-1 update is applied to the
+// panel's remaining columns. Returns j + 1 for a zero pivot (the reference throws).
+template<class T>
+size_t getrf_panel(size_t rows, size_t cols, View<T> A, int* piv) {
+	for (size_t j = 0; j < cols; ++j) {
+		double pv = A(j, j);
+		piv[j] = (int)j;
+		for (size_t i = j + 1; i < rows; ++i)
+			if (std::abs((double)A(i, j)) > std::abs(pv)) {
+				piv[j] = (int)i;
+				pv = A(i, j);
+			}
+		if (pv == 0) return j + 1;
+		if ((size_t)piv[j] != j)
+			for (size_t c = 0; c < cols; ++c) std::swap(A(j, c), A((size_t)piv[j], c));
+		for (size_t i = j + 1; i < rows; ++i) A(i, j) = (T)(A(i, j) / pv);
+		for (size_t k = j + 1; k < cols; ++k)
+			for (size_t i = j + 1; i < rows; ++i) A(i, k) -= A(i, j) * A(j, k);
+	}
+	return 0;
+}
+
+// getrf_recursive: kernels/default/getrf.hpp:117-166 -- columns [start, end) of the n x n A,
+// split at a multiple of 4 columns: left half recursively, its row swaps applied to the
+// right half's columns, A12 <- L11^-1 A12 (unit lower), A22 -= A21 A12, right half
+// recursively, its row swaps applied to A21 and its pivots made relative to `start`.
+template<class T>
+size_t getrf_rec(size_t n, View<T> A, int* piv, size_t start, size_t end) {
+	const size_t block = 4, size = end - start, rows = n - start;
+	if (size <= block) {
+		const size_t r = getrf_panel<T>(rows, size, A.sub(start, start), piv + start);
+		return r ? r + start : 0;
+	}
+	const size_t split = start + (size + block - 1) / block / 2 * block;
+	size_t r = getrf_rec<T>(n, A, piv, start, split);
+	if (r) return r;
+	swap_rows_seq<T>(split - start, piv + start, end - split, A.sub(start, split));
+	View<const T> L11{A.sub(start, start).p, A.rs, A.cs};
+	trsm<T>(true, false, true, split - start, end - split, L11, A.sub(start, split));
+	View<const T> A21{A.sub(split, start).p, A.rs, A.cs}, A12{A.sub(start, split).p, A.rs, A.cs};
+	gemm<T>(n - split, end - split, split - start, T(-1), A21, A12, A.sub(split, split));
+	if ((r = getrf_rec<T>(n, A, piv, split, end))) return r;
+	swap_rows_seq<T>(end - split, piv + split, split - start, A.sub(split, start));
+	for (size_t i = split; i < end; ++i) piv[i] += (int)(split - start);
+	return 0;
+}
+
+// pstrf (lower): kernels/default/pstrf.hpp:40-147, the blocked pivoted Cholesky of LAWN 161
+// with blocks of 20 columns. Inside a block the pivot values (the diagonal of the updated
+// trailing matrix) are refreshed from the block's finished columns; the largest remaining
+// one (first of equals) is swapped into place, rows and columns of the whole matrix; the
+// factor stops with rank k + j once a pivot value falls below n^2 eps max|A_ii| (the
+// trailing square is cleared); each column is finished by a gemv against the block's
+// earlier columns and a division; the row right of the diagonal is cleared; after the
+// block, the trailing square is updated with the block's columns. piv[i] is set only where
+// a swap happens (callers start from the identity). Returns the rank.
+template<class T>
+size_t pstrf_lower(size_t m, View<T> A, int* piv) {
+	const size_t block = 20;
+	double max_diag = A(0, 0);
+	for (size_t i = 1; i < m; ++i) max_diag = std::max(max_diag, (double)std::abs(A(i, i)));
+	const double eps = (double)(m * m) * std::numeric_limits<T>::epsilon() * max_diag;
+	std::vector<T> pv(m);
+	for (size_t k = 0; k < m; k += block) {
+		const size_t cur = std::min(m - k, block), rest = m - k;
+		View<T> Ak = A.sub(k, k);
+		for (size_t j = 0; j < cur; ++j) {
+			if (j == 0) {
+				for (size_t i = 0; i < rest; ++i) pv[i] = Ak(i, i);
+			} else {
+				for (size_t i = j; i < rest; ++i) pv[i] -= Ak(i, j - 1) * Ak(i, j - 1);
+			}
+			size_t p = j;
+			for (size_t i = j + 1; i < rest; ++i)
+				if (pv[i] > pv[p]) p = i;
+			if (p != j) {
+				piv[k + j] = (int)(k + p);
+				for (size_t c = 0; c < m; ++c) std::swap(A(k + j, c), A(k + p, c));
+				for (size_t r = 0; r < m; ++r) std::swap(A(r, k + j), A(r, k + p));
+				std::swap(pv[j], pv[p]);
+			}
+			const T v = pv[j];
+			if (v < eps) {
+				for (size_t i = j; i < rest; ++i)
+					for (size_t c = j; c < rest; ++c) Ak(i, c) = T(0);
+				return k + j;
+			}
+			Ak(j, j) = std::sqrt(v);
+			if (j > 0) {
+				std::vector<T> row(j);
+				for (size_t c = 0; c < j; ++c) row[c] = Ak(j, c);
+				View<const T> LL{Ak.sub(j + 1, 0).p, Ak.rs, Ak.cs};
+				gemv<T>(rest - j - 1, j, T(-1), LL, row.data(), 1, &Ak(j + 1, j), Ak.rs);
+			}
+			for (size_t i = j + 1; i < rest; ++i) Ak(i, j) /= Ak(j, j);
+			for (size_t c = j + 1; c < rest; ++c) Ak(j, c) = T(0);
+		}
+		if (k + cur < m) {
+			View<const T> LL{Ak.sub(block, 0).p, Ak.rs, Ak.cs};
+			gemm<T>(rest - block, rest - block, block, T(-1), LL, LL.t(), Ak.sub(block, block));
+		}
+	}
+	return m;
+}
+
 }  // namespace
 
 extern "C" {
@@ -334,6 +456,22 @@ size_t orc_potrf_f64(int upper, size_t n, double* A, ptrdiff_t rs, ptrdiff_t cs)
 }
 size_t orc_potrf_f32(int upper, size_t n, float* A, ptrdiff_t rs, ptrdiff_t cs) {
 	return potrf<float>(upper, n, {A, rs, cs});
+}
+size_t orc_getrf_f64(size_t n, double* A, ptrdiff_t rs, ptrdiff_t cs, int* piv) {
+	for (size_t i = 0; i < n; ++i) piv[i] = (int)i;
+	return getrf_rec<double>(n, {A, rs, cs}, piv, 0, n);
+}
+size_t orc_getrf_f32(size_t n, float* A, ptrdiff_t rs, ptrdiff_t cs, int* piv) {
+	for (size_t i = 0; i < n; ++i) piv[i] = (int)i;
+	return getrf_rec<float>(n, {A, rs, cs}, piv, 0, n);
+}
+size_t orc_pstrf_f64(size_t n, double* A, ptrdiff_t rs, ptrdiff_t cs, int* piv) {
+	for (size_t i = 0; i < n; ++i) piv[i] = (int)i;
+	return n ? pstrf_lower<double>(n, {A, rs, cs}, piv) : 0;
+}
+size_t orc_pstrf_f32(size_t n, float* A, ptrdiff_t rs, ptrdiff_t cs, int* piv) {
+	for (size_t i = 0; i < n; ++i) piv[i] = (int)i;
+	return n ? pstrf_lower<float>(n, {A, rs, cs}, piv) : 0;
 }
 size_t orc_cholesky_solve_f64(size_t n, size_t nrhs, const double* A, ptrdiff_t ars, ptrdiff_t acs,
                               double* B, ptrdiff_t brs, ptrdiff_t bcs) {

@@ -81,6 +81,16 @@ void orc_trmm_f32(int upper, int unit, size_t m, size_t n, const float* A, ptrdi
  * left untouched. Returns 0, or the 1-based GLOBAL index of the first non-positive pivot. */
 size_t orc_potrf_f64(int upper, size_t n, double* A, ptrdiff_t rs, ptrdiff_t cs);
 size_t orc_potrf_f32(int upper, size_t n, float* A, ptrdiff_t rs, ptrdiff_t cs);
+/* LU with partial pivoting in place (unit lower L below the diagonal, U on and above):
+ * piv[i] = the row swapped with row i, in order i = 0, 1, ... (kernels/getrf.hpp:50-59).
+ * Returns 0, or the 1-based column of the first zero pivot (the reference throws). */
+size_t orc_getrf_f64(size_t n, double* A, ptrdiff_t rs, ptrdiff_t cs, int* piv);
+size_t orc_getrf_f32(size_t n, float* A, ptrdiff_t rs, ptrdiff_t cs, int* piv);
+/* Pivoted Cholesky P^T A P = L L^T of a symmetric positive semidefinite A, L in the lower
+ * triangle (zeros above), piv as for getrf (kernels/pstrf.hpp:62-70); returns the rank,
+ * the columns from the rank on are zero. */
+size_t orc_pstrf_f64(size_t n, double* A, ptrdiff_t rs, ptrdiff_t cs, int* piv);
+size_t orc_pstrf_f32(size_t n, float* A, ptrdiff_t rs, ptrdiff_t cs, int* piv);
 /* cholesky_decomposition(A).solve(B, left): A n x n SPD (lower triangle read), B n x nrhs.
  * Returns the potrf status. A is not modified. */
 size_t orc_cholesky_solve_f64(size_t n, size_t nrhs, const double* A, ptrdiff_t ars, ptrdiff_t acs,

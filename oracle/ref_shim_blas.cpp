@@ -15,6 +15,8 @@
 //   kernels::trmv<Upper,Unit>(A,b)    include/remora/kernels/trmv.hpp:54-65
 //   kernels::trmm<Upper,Unit>(A,B)    include/remora/kernels/trmm.hpp:53-64
 //   cholesky_decomposition + solve    include/remora/decompositions.hpp:70-115
+//   kernels::getrf(A,P)               include/remora/kernels/getrf.hpp:50-59
+//   kernels::pstrf<lower>(A,P)        include/remora/kernels/pstrf.hpp:62-70
 //   kernels::generate_normal/uniform/discrete (CPU input generator)
 //                                     include/remora/kernels/default/random.hpp:37-122
 #include <remora/remora.hpp>
@@ -225,6 +227,34 @@ void trmm_all(int upper, int unit, int a_rm, int b_rm, std::size_t m, std::size_
 	else if (b_rm) trmm_tri<T, column_major, row_major>(upper, unit, m, n, A, lda, B, ldb);
 	else trmm_tri<T, column_major, column_major>(upper, unit, m, n, A, lda, B, ldb);
 }
+// kernels::getrf / kernels::pstrf take matrix containers too: copy in and out. P starts as
+// the identity (permutation_matrix); getrf's "rank deficient" exception becomes -1.
+template<class T, class O>
+long getrf_impl(std::size_t n, T* A, std::size_t ld, int* P) {
+	view<T, O> a(A, n, n, ld);
+	matrix<T, O> m = a;
+	permutation_matrix p(n);
+	try {
+		kernels::getrf(m, p);
+	} catch (std::invalid_argument const&) {
+		return -1;
+	}
+	noalias(a) = m;
+	for (std::size_t i = 0; i != n; ++i) P[i] = p(i);
+	return 0;
+}
+
+template<class T, class O>
+std::size_t pstrf_impl(std::size_t n, T* A, std::size_t ld, int* P) {
+	view<T, O> a(A, n, n, ld);
+	matrix<T, O> m = a;
+	permutation_matrix p(n);
+	std::size_t rank = kernels::pstrf<remora::lower>(m, p);
+	noalias(a) = m;
+	for (std::size_t i = 0; i != n; ++i) P[i] = p(i);
+	return rank;
+}
+
 }  // namespace
 
 extern "C" {
@@ -244,6 +274,19 @@ std::size_t ref_potrf_f32(int upper, int row_major_, std::size_t n, float* A, st
 	if (!row_major_ && upper) return potrf_impl<float, column_major, remora::upper>(n, A, ld);
 	return (std::size_t)-1;
 }
+
+long ref_getrf_f64(int row_major_, std::size_t n, double* A, std::size_t ld, int* P) {
+	return row_major_ ? getrf_impl<double, row_major>(n, A, ld, P) : getrf_impl<double, column_major>(n, A, ld, P);
+}
+long ref_getrf_f32(int row_major_, std::size_t n, float* A, std::size_t ld, int* P) {
+	return row_major_ ? getrf_impl<float, row_major>(n, A, ld, P) : getrf_impl<float, column_major>(n, A, ld, P);
+}
+std::size_t ref_pstrf_f64(int row_major_, std::size_t n, double* A, std::size_t ld, int* P) {
+	return row_major_ ? pstrf_impl<double, row_major>(n, A, ld, P) : pstrf_impl<double, column_major>(n, A, ld, P);
+}
+// FP32 pstrf does not compile in the reference (kernels/default/pstrf.hpp:78 calls
+// std::max(double&, float)): (size_t)-1.
+std::size_t ref_pstrf_f32(int, std::size_t, float*, std::size_t, int*) { return (std::size_t)-1; }
 
 int ref_trsm_f64(int left, int upper, int unit, int a_rm, int b_rm, std::size_t m, std::size_t n,
                  double const* A, std::size_t lda, double* B, std::size_t ldb) {

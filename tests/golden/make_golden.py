@@ -164,6 +164,60 @@ def blas2_fixture(ref: oracle.Reference) -> None:
     np.savez_compressed(OUT / "blas2.npz", **res)
 
 
+def lu_input(n: int) -> np.ndarray:
+    """The getrf test matrix of Test/getrf.cpp:15-33: L U with L(i, j) = 3 - 3 |i - j| / n
+    below a unit diagonal and U = diag(1 + i / (2 n)), built so that partial pivoting
+    moves to the next row at every step."""
+    L = np.eye(n)
+    for i in range(n):
+        for j in range(i):
+            L[i, j] = 3 - 3.0 / n * abs(i - j)
+    return L @ np.diag(0.5 / n * np.arange(n) + 1)
+
+
+def semidef_input(n: int, rank: int = 0) -> np.ndarray:
+    """The pivoted-Cholesky test matrix of Test/symm_solve.cpp:17-38: R R^T with
+    R(i, j) = 0.2 / |i - j| (j < min(i, rank)), R(i, i) = 1 + i / (2 n) for i < rank, and
+    for rank < n the rows and columns 2 i and n - 1 - i swapped (i < rank / 2)."""
+    rank = rank or n
+    R = np.zeros((n, n))
+    for i in range(n):
+        for j in range(min(i, rank)):
+            R[i, j] = 0.2 / abs(i - j)
+        if i < rank:
+            R[i, i] = 0.5 / n * i + 1
+    A = R @ R.T
+    if rank != n:
+        for i in range(rank // 2):
+            a, b = 2 * i, n - i - 1
+            A[[a, b]] = A[[b, a]]
+            A[:, [a, b]] = A[:, [b, a]]
+    return A
+
+
+def lu_pstrf_fixture(ref: oracle.Reference) -> None:
+    # kernels::getrf on the Test/getrf.cpp matrix (n = 123) and on a U[-1, 1] matrix from the
+    # reference CPU generator (n = 61); kernels::pstrf<lower> on the Test/symm_solve.cpp
+    # matrix at full rank (60) and rank-deficient (57 of rank 25, 45 of rank 44). Row-major
+    # runs; for pstrf the pivot recorded at the rank itself picks among rounding-level
+    # remainders and is not part of the parity contract.
+    res = {}
+    g = ref.rng(11)
+    cases = {"lu123": lu_input(123), "lu61": g.uniform(61, 61, -1.0, 1.0)}
+    for name, A in cases.items():
+        F = np.array(A, order="C")
+        st, piv = ref.getrf(F)
+        assert st == 0
+        res[f"{name}_A"], res[f"{name}_F"], res[f"{name}_piv"] = A, F, piv
+    for name, (n, r) in {"ps60": (60, 0), "ps57r25": (57, 25), "ps45r44": (45, 44)}.items():
+        A = semidef_input(n, r)
+        F = np.array(A, order="C")
+        rank, piv = ref.pstrf(F)
+        res[f"{name}_A"], res[f"{name}_F"], res[f"{name}_piv"] = A, F, piv
+        res[f"{name}_rank"] = np.array(rank)
+    np.savez_compressed(OUT / "lu_pstrf.npz", **res)
+
+
 def solve_fixture(ref: oracle.Reference) -> None:
     # The n = 1024 SPD solve recipe at n = 48: G ~ N(0,1) from mt19937(seed) through the
     # reference CPU generator, A = G G^T / n + 1e-2 I (reference gemm), B ~ N(0,1).
@@ -189,6 +243,7 @@ def main() -> None:
     syrk_gemm_fixture(ref)
     blas2_fixture(ref)
     solve_fixture(ref)
+    lu_pstrf_fixture(ref)
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

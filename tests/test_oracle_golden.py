@@ -130,6 +130,66 @@ def test_blas2(orc, golden):
             assert oracle.rel_fro(X, g[f"trmm_u{upper}_d{unit}"]) <= 1e-14
 
 
+def _apply_swaps(A: np.ndarray, piv: np.ndarray, cols: bool) -> np.ndarray:
+    """Row swaps i <-> piv[i] in order i = 0, 1, ... (and the same column swaps)."""
+    B = A.copy()
+    for i, p in enumerate(piv):
+        if p != i:
+            B[[i, p]] = B[[p, i]]
+            if cols:
+                B[:, [i, p]] = B[:, [p, i]]
+    return B
+
+
+@pytest.mark.parametrize("name", ["lu123", "lu61"])
+@pytest.mark.parametrize("order", ["C", "F"])
+def test_getrf(orc, golden, name, order):
+    """LU with partial pivoting: the same pivots as the reference's kernels::getrf, factors
+    within 1e-13, and P L U = A."""
+    g = golden("lu_pstrf")
+    A = g[f"{name}_A"]
+    F = np.array(A, order=order)
+    st, piv = orc.getrf(F)
+    assert st == 0
+    assert np.array_equal(piv, g[f"{name}_piv"])
+    assert oracle.rel_fro(F, g[f"{name}_F"]) <= 1e-13
+    L, U = np.tril(F, -1) + np.eye(len(piv)), np.triu(F)
+    assert oracle.rel_fro(L @ U, _apply_swaps(A, piv, cols=False)) <= 1e-13
+
+
+def test_getrf_f32_and_singular(orc):
+    rs = np.random.default_rng(2)
+    A = rs.uniform(-1, 1, (50, 50))
+    F32 = np.array(A, dtype=np.float32)
+    st, piv = orc.getrf(F32)
+    F64 = A.copy()
+    assert st == 0 and orc.getrf(F64)[0] == 0
+    assert oracle.rel_fro(F32, F64) <= 1e-5
+    S = A.copy()
+    S[:, 7] = 0.0  # a zero column: the pivot search of column 7 finds only zeros
+    assert orc.getrf(S)[0] == 8
+
+
+@pytest.mark.parametrize("name", ["ps60", "ps57r25", "ps45r44"])
+@pytest.mark.parametrize("order", ["C", "F"])
+def test_pstrf(orc, golden, name, order):
+    """Pivoted Cholesky against the reference's kernels::pstrf<lower>: the same rank, the
+    same pivots before the rank, the same diagonal of L, and P^T A P = L L^T. (At the rank
+    itself the reference swaps in the largest of the rounding-level remainders before it
+    stops, so that one pivot depends on the summation order.)"""
+    g = golden("lu_pstrf")
+    A = g[f"{name}_A"]
+    F = np.array(A, order=order)
+    rank, piv = orc.pstrf(F)
+    r = int(g[f"{name}_rank"])
+    assert rank == r
+    assert np.array_equal(piv[:r], g[f"{name}_piv"][:r])
+    d, dref = np.diag(F)[:r], np.diag(g[f"{name}_F"])[:r]
+    assert np.max(np.abs(d - dref) / dref) <= 1e-13
+    assert np.all(np.triu(F, 1) == 0.0) and np.all(F[:, r:] == 0.0)
+    assert oracle.rel_fro(F @ F.T, _apply_swaps(A, piv, cols=True)) <= 1e-13
+
+
 def test_cholesky_solve(orc, golden):
     g = golden("solve")
     X = np.array(g["B"], order="F")
