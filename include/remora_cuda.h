@@ -232,9 +232,13 @@ int rc_batched_release_plans(void);
  *  - factor S A S + theta I (S = diag(A)^-1/2, theta a multiple of u_f) in FP32 storage
  *    with FP64 diagonal blocks and TF32 or BF16 tensor-core trailing updates (FP32
  *    accumulation);
- *  - refine in FP64 (FP64 residuals and products) by preconditioned conjugate gradients
- *    with that factor, per right-hand side, until the normwise backward error
- *    ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol on every column.
+ *  - refine in FP64 by preconditioned conjugate gradients with that factor, per
+ *    right-hand side, until the normwise backward error
+ *    ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol on every column. With at
+ *    most 64 right-hand sides and n >= 512, the CG products A p run on the int8 tensor
+ *    cores on an exact digit split of A (as rc_gemm_f64_sliced, rows and columns scaled
+ *    from the diagonal), which adds 8 n^2 bytes to the workspace; every residual that
+ *    decides convergence is an FP64 DMMA product.
  * The call synchronises the stream (convergence is decided on the host). Returns
  * RC_ERR_NOT_CONVERGED when max_iter is reached first; d_info receives the failing pivot
  * when the low-precision factorisation breaks down (then X is not written). */

@@ -953,7 +953,6 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     cudaEvent_t e0, e1, e2;
     cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
     cudaEventRecord(e0, s);
-    // The digit split of A runs on a background stream while A is factored.
     const View<const double> Av = M.Av();
     diag_scale_kernel<<<ceil_div(n, 256) < 1024u ? ceil_div(n, 256) : 1024u, 256, 0, s>>>(n, Av, M.sc);
     RC_TRY(check_launch());
