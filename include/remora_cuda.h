@@ -189,6 +189,25 @@ int rc_trmv_f32(int upper, int trans, int unit, size_t n, const float* A, size_t
 int rc_potrf_f64(int upper, size_t n, double* A, size_t lda, int* d_info, void* stream);
 int rc_potrf_f32(int upper, size_t n, float* A, size_t lda, int* d_info, void* stream);
 
+/* LU with partial pivoting in place on the n x n matrix A (column-major; row-major when
+ * row_major = 1): A = P L U, L unit lower below the diagonal, U on and above it.
+ * d_piv (device, n ints): the row swapped with row i at step i, 0-based, applied in the
+ * order i = 0, 1, ... (Remora's permutation_matrix). d_info (device): 0, or the 1-based
+ * column of the first zero pivot, where the factorisation stops (the reference throws).
+ * Replaces kernels::getrf (include/remora/kernels/getrf.hpp:50-59; CPU algorithm
+ * kernels/default/getrf.hpp:41-181). */
+int rc_getrf_f64(int row_major, size_t n, double* A, size_t lda, int* d_piv, int* d_info, void* stream);
+int rc_getrf_f32(int row_major, size_t n, float* A, size_t lda, int* d_piv, int* d_info, void* stream);
+
+/* Pivoted Cholesky P^T A P = L L^T of the symmetric positive semidefinite n x n A in place:
+ * L in the lower triangle, zeros above it and in the columns from the rank on. d_piv as
+ * for rc_getrf (identity where no swap happened); *d_rank (device) = the rank: the
+ * factorisation stops once the largest remaining pivot is below n^2 eps max|A_ii|.
+ * Replaces kernels::pstrf<lower> (include/remora/kernels/pstrf.hpp:62-70; CPU algorithm
+ * kernels/default/pstrf.hpp:40-147). */
+int rc_pstrf_f64(int row_major, size_t n, double* A, size_t lda, int* d_piv, int* d_rank, void* stream);
+int rc_pstrf_f32(int row_major, size_t n, float* A, size_t lda, int* d_piv, int* d_rank, void* stream);
+
 /* X = A^-1 B for SPD A via Cholesky: cholesky_decomposition(A).solve(B, left())
  * (include/remora/decompositions.hpp:81-84, :101-105; solve.hpp:165-170). A (n x n,
  * lower triangle read) is not modified; B (n x nrhs) is overwritten with X. d_info as

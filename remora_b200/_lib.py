@@ -75,6 +75,10 @@ SIGNATURES: dict[str, list] = {
     "rc_axpby_f64": [_Z, c_double, _P, _Z, c_double, _P, _Z, _P],
     "rc_axpby_f32": [_Z, c_float, _P, _Z, c_float, _P, _Z, _P],
     "rc_potrf_f64": [_I, _Z, _P, _Z, _P, _P],
+    "rc_getrf_f64": [_I, _Z, _P, _Z, _P, _P, _P],
+    "rc_getrf_f32": [_I, _Z, _P, _Z, _P, _P, _P],
+    "rc_pstrf_f64": [_I, _Z, _P, _Z, _P, _P, _P],
+    "rc_pstrf_f32": [_I, _Z, _P, _Z, _P, _P, _P],
     "rc_potrf_f32": [_I, _Z, _P, _Z, _P, _P],
     "rc_spd_solve_f64": [_Z, _Z, _P, _Z, _P, _Z, _P, _P],
     "rc_spd_solve_f64_noalloc": [_Z, _Z, _P, _Z, _P, _Z, _P, _P],

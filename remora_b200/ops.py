@@ -136,6 +136,29 @@ def potrf(A: torch.Tensor, upper: bool = False, info: torch.Tensor | None = None
     return int(info.item()) if sync else info
 
 
+def getrf(A: torch.Tensor) -> tuple[int, torch.Tensor]:
+    """LU with partial pivoting in place (A = P L U); returns (info, piv): info 0 or the
+    1-based column of the first zero pivot, piv the device int32 swap sequence."""
+    sfx = _sfx(A)
+    n = A.shape[0]
+    ta, lda = layout(A)
+    piv = torch.empty(n, dtype=torch.int32, device=A.device)
+    info = torch.zeros(1, dtype=torch.int32, device=A.device)
+    call(f"rc_getrf_{sfx}", ta, n, _ptr(A), lda, _ptr(piv), _ptr(info), _stream())
+    return int(info.item()), piv
+
+
+def pstrf(A: torch.Tensor) -> tuple[int, torch.Tensor]:
+    """Pivoted Cholesky P^T A P = L L^T in place (L lower); returns (rank, piv)."""
+    sfx = _sfx(A)
+    n = A.shape[0]
+    ta, lda = layout(A)
+    piv = torch.empty(n, dtype=torch.int32, device=A.device)
+    rank = torch.zeros(1, dtype=torch.int32, device=A.device)
+    call(f"rc_pstrf_{sfx}", ta, n, _ptr(A), lda, _ptr(piv), _ptr(rank), _stream())
+    return int(rank.item()), piv
+
+
 def cholesky_solve(A: torch.Tensor, B: torch.Tensor, info: torch.Tensor | None = None) -> int:
     """B <- A^-1 B for SPD A (FP64; A's lower triangle read, A unchanged)."""
     if A.dtype != torch.float64 or B.dtype != torch.float64:
