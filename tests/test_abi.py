@@ -52,3 +52,17 @@ def test_argument_checks_need_no_device():
     assert lib.rc_rng_discrete_i32(key, 4, 4, fake, 4, 1, 5, 2, None) == 1
     # empty problems are no-ops
     assert lib.rc_gemm_f32(0, 0, 0, 5, 5, 1.0, None, 1, None, 1, 0.0, None, 1, None) == 0
+
+
+def test_argument_checks_of_factorisations_and_sliced_product():
+    """getrf / pstrf / the int8 FP64 product reject bad arguments before any CUDA call."""
+    lib = remora_b200.lib()
+    fake = ctypes.c_void_p(16)
+    assert lib.rc_getrf_f64(0, 10, fake, 10, fake, None, None) == 1  # no status word
+    assert lib.rc_getrf_f32(1, 10, fake, 5, fake, fake, None) == 1  # lda < n
+    assert lib.rc_pstrf_f64(0, 10, fake, 10, fake, None, None) == 1  # no rank word
+    assert lib.rc_pstrf_f32(0, 10, None, 10, fake, fake, None) == 1  # no matrix
+    assert lib.rc_gemm_f64_sliced(10, 4, 10, 1.0, None, 10, fake, 10, 0.0, fake, 10, None) == 1
+    assert lib.rc_gemm_f64_sliced(10, 4, 10, 1.0, fake, 9, fake, 10, 0.0, fake, 10, None) == 1  # lda < m
+    assert lib.rc_gemm_f64_sliced(10, 65, 10, 1.0, fake, 10, fake, 10, 0.0, fake, 10, None) == 4  # > 64 columns
+    assert lib.rc_gemm_f64_sliced(0, 4, 10, 1.0, None, 1, None, 1, 0.0, None, 1, None) == 0  # empty
