@@ -144,11 +144,23 @@ def cpu_reference(n: int, nrhs: int, steps: int, warmup: int, seed: int = 1) -> 
 
 
 def workload_config(args, world: int) -> dict:
-    """The config both arms report: the headline workload they are measured on."""
+    """The config of this build's arm: the headline workload it is measured on."""
     return {"workload": f"mixed-precision refined SPD solve n={args.n} nrhs={args.nrhs} kappa={args.kappa:g}",
             "n": args.n, "nrhs": args.nrhs, "kappa": args.kappa, "precision": args.precision,
             "tol": 1e-15, "parallelism": f"replicas x{world}",
             "l2": "inputs larger than L2 (A is n^2 x 8 bytes)"}
+
+
+def reference_config(args) -> dict:
+    """The config of the reference arm: the work its timer actually measures -- an FP64 CPU
+    solve at the sample size, a bounded stand-in for the n x n headline solve, counted in
+    the same metric unit (n^3/3 + 2 n^2 nrhs of the sample's own n)."""
+    return {"workload": f"Remora CPU cholesky_decomposition + solve, FP64, n={args.ref_n} nrhs={args.nrhs} "
+                        f"(bounded sample of the n={args.n} headline solve; the CPU rate is flat in n "
+                        f"above ~2048)",
+            "n": args.ref_n, "nrhs": args.nrhs, "kappa": None, "precision": None, "arithmetic": "fp64 (CPU)",
+            "headline_n": args.n, "parallelism": "1 host thread (the reference is single-threaded)",
+            "l2": "n/a (CPU)"}
 
 
 def run_reference_arm(args) -> None:
@@ -160,8 +172,9 @@ def run_reference_arm(args) -> None:
     line = {
         "metric": METRIC, "value": r["value"], "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args, 1),
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (G G^T / n + 1e-2 I from Remora's mt19937 "
+                                                        "generator, N(0,1) right-hand sides)",
+        "config": reference_config(args),
         "impl": "reference",
         "cpu_baseline": {"value": r["value"], "unit": "TFLOP/s", "cores": 1, "kind": "reference",
                          "sample": f"Remora's CPU cholesky_decomposition + solve (FP64), one n={n}, "
@@ -186,11 +199,43 @@ def max_over_ranks(value: float, device=None) -> float:
 
 
 _T0 = time.perf_counter()
+_PHASE = ["start"]
 
 
 def phase(name: str) -> None:
     """Progress of the default run on stderr (the JSON result line is the only stdout)."""
+    _PHASE[0] = name
     print(f"[bench {time.perf_counter() - _T0:7.1f} s] {name}", file=sys.stderr, flush=True)
+
+
+def start_watchdog(seconds: float) -> None:
+    """End the process (exit status 3, with the phase it was in) if the run outlives
+    `seconds`: a stalled run then fails in minutes instead of holding the GPU until an
+    outer limit kills it. Every device wait of the library is bounded, so this is the last
+    line, not the first."""
+    import threading
+
+    def fire():
+        print(json.dumps({"metric": METRIC, "error": f"watchdog: no result after {seconds:.0f} s",
+                          "phase": _PHASE[0]}), flush=True)
+        print(f"[bench] watchdog fired in phase '{_PHASE[0]}'", file=sys.stderr, flush=True)
+        os._exit(3)
+
+    t = threading.Timer(seconds, fire)
+    t.daemon = True
+    t.start()
+
+
+def fail_on_status(lib, status: int, info: dict, where: str) -> None:
+    """A solve that did not succeed ends the run with its status and, for a device
+    timeout, the site of the wait that ran out."""
+    if status == 0:
+        return
+    site = ctypes.c_int(0)
+    dev_status = lib.rc_device_error_site(None, ctypes.byref(site))
+    print(json.dumps({"metric": METRIC, "error": f"{where}: rc_spd_solve_mixed returned {status}",
+                      "device_status": dev_status, "timeout_site": site.value, "info": info}), flush=True)
+    sys.exit(4)
 
 
 def run_ours(args) -> None:
@@ -225,8 +270,9 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
 
     phase("warm-up")
-    for _ in range(args.warmup):
+    for i in range(args.warmup):
         info, status = step()
+        fail_on_status(lib, status, info, f"warm-up step {i}")
     barrier()
     phase("timed steps")
     launches0 = lib.rc_launch_count()
@@ -240,6 +286,8 @@ def run_ours(args) -> None:
         e1.record(stream)
         barrier()
     launches = lib.rc_launch_count() - launches0
+    for i, (info_i, status_i) in enumerate(infos):
+        fail_on_status(lib, status_i, info_i, f"timed step {i}")
     t = max_over_ranks(e0.elapsed_time(e1) / 1e3, dev)
     mixed_bwd = backward_error(A, X, B)
     status_ok = all(s == 0 for _, s in infos)
@@ -283,13 +331,16 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
         barrier()
         e0.record(stream)
+        statuses = []
         for _ in range(args.steps):
             Ad.copy_(Ah, non_blocking=True)
             Bd.copy_(Bh, non_blocking=True)
-            ops.spd_solve_mixed(Ad, Bd, args.precision, tol=1e-15, max_iter=args.max_iter, X=X)
+            statuses.append(ops.spd_solve_mixed(Ad, Bd, args.precision, tol=1e-15, max_iter=args.max_iter, X=X)[1:])
             Xh.copy_(X, non_blocking=True)
         e1.record(stream)
         barrier()
+        for i, (info_i, status_i) in enumerate(statuses):
+            fail_on_status(lib, status_i, info_i, f"end-to-end step {i}")
         te = max_over_ranks(e0.elapsed_time(e1) / 1e3, dev)
         e2e = {"value": world * args.steps * flops(n, nrhs) / te / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": n * n * 8 + n * nrhs * 8, "d2h_bytes_per_step": n * nrhs * 8,
@@ -468,7 +519,11 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--case", choices=["syrk_tc", "dgemm", "potrf", "rng", "mixed", "batched", "sliced"],
                     help="run one small kernel case (for ncu captures) instead of the benchmark")
+    ap.add_argument("--watchdog", type=float, default=900.0,
+                    help="seconds after which a run that has not finished exits with status 3")
     args = ap.parse_args()
+    if args.watchdog > 0:
+        start_watchdog(args.watchdog)
     if args.case:
         run_case(args)
     elif args.impl == "reference":

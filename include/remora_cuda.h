@@ -42,15 +42,22 @@ const char* rc_error_string(int status);
 unsigned long long rc_launch_count(void);
 /* Free every cached workspace of the current device (synchronises the device). */
 int rc_release_workspaces(void);
-/* Failure detection. Every device-side wait (mbarrier phases of the tensor-core
- * pipelines, the batched solver's cross-CTA flags) is bounded by a wall-clock limit
- * (default 2 s); a wait that runs out records RC_ERR_TIMEOUT in a per-device error word
- * and its kernel returns, leaving the context usable. rc_device_status synchronises the
- * stream and returns (then clears) that word. rc_selftest_wait_timeout launches one
- * bounded wait on a barrier that nothing completes, to exercise that path. These have
- * no reference counterpart (the reference checks no launch, hip/exception.hpp:41-63). */
+/* Failure detection. Every device-side wait (the mbarrier phases of the tensor-core
+ * pipelines) is bounded: by the SM's cycle counter, 2 cycles per nanosecond of the limit
+ * set here (default 2 s), i.e. at least that long at SM clocks up to 2 GHz. A wait that
+ * runs out records RC_ERR_TIMEOUT and where it happened (kernel * 100 + role * 10 + CTA
+ * rank in its cluster; kernels 1 = tcgen05 GEMM, 2 = CTA-pair GEMM, 3 = int8 product,
+ * 9 = self-test; roles 0 = loads, 1 = MMAs, 2 = epilogue) in a per-device error word and
+ * its kernel returns, leaving the context usable. The word is sticky: while it is set,
+ * every tensor-core kernel returns at once and waits in flight give up, and
+ * rc_spd_solve_mixed returns RC_ERR_TIMEOUT. rc_device_status synchronises the stream
+ * and returns (then clears) the status; rc_device_error_site also writes the site.
+ * rc_selftest_wait_timeout launches one bounded wait on a barrier that nothing
+ * completes, to exercise that path. These have no reference counterpart (the reference
+ * checks no launch, hip/exception.hpp:41-63). */
 int rc_set_wait_limit_ns(uint64_t ns);
 int rc_device_status(void* stream);
+int rc_device_error_site(void* stream, int* site);
 int rc_selftest_wait_timeout(uint64_t limit_ns, void* stream);
 
 /* ---------------------------------------------------------------------------------

@@ -10,6 +10,7 @@ and only as the checker / the timed CPU baseline. The product never imports it.
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 from ctypes import POINTER, c_double, c_float, c_int, c_size_t, c_ssize_t, c_uint32, c_uint64, c_void_p
 from pathlib import Path
@@ -19,14 +20,23 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "liboracle.so"
 REF_SO = HERE / "_ref" / "libremora_ref.so"
+# Where the reference's headers lie (include/ of the Remora source tree): the environment
+# variable REMORA_REF_INCLUDE, else the default of oracle/Makefile.
+REF_INCLUDE = Path(os.environ.get("REMORA_REF_INCLUDE", "/root/reference/include"))
+
+
+def reference_present() -> bool:
+    """True where Remora's headers are on this machine (not on a machine that only runs the
+    prebuilt libraries)."""
+    return (REF_INCLUDE / "remora").is_dir()
 _U4 = c_uint32 * 4
 
 
 def build(ref: bool = True) -> None:
     """Compile the oracle (always) and the reference CPU shim (when its headers exist)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
-    if ref and Path("/root/reference/include/remora").is_dir():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+    if ref and reference_present():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_INCLUDE={REF_INCLUDE}"], check=True)
 
 
 def _p(a: np.ndarray) -> c_void_p:

@@ -59,6 +59,7 @@ SIGNATURES: dict[str, list] = {
     "rc_gemm_bf16": [_I, _I, _Z, _Z, _Z, c_float, _P, _Z, _P, _Z, c_float, _P, _Z, _P],
     "rc_set_wait_limit_ns": [ctypes.c_uint64],
     "rc_device_status": [_P],
+    "rc_device_error_site": [_P, _P],
     "rc_selftest_wait_timeout": [ctypes.c_uint64, _P],
     "rc_syrk_f64": [_I, _I, _Z, _Z, c_double, _P, _Z, c_double, _P, _Z, _P],
     "rc_syrk_f32": [_I, _I, _Z, _Z, c_float, _P, _Z, c_float, _P, _Z, _P],

@@ -67,13 +67,23 @@ int* error_word() {
     if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
     std::lock_guard<std::mutex> lock(g_mutex);
     int*& w = g_error_words[dev];
-    if (!w) {
-        if (cudaMalloc(&w, sizeof(int)) != cudaSuccess || cudaMemset(w, 0, sizeof(int)) != cudaSuccess) {
+    if (!w) {  // [status, site of the first timeout]
+        if (cudaMalloc(&w, 2 * sizeof(int)) != cudaSuccess || cudaMemset(w, 0, 2 * sizeof(int)) != cudaSuccess) {
             cudaGetLastError();
             w = nullptr;
         }
     }
     return w;
+}
+
+int pending_error(cudaStream_t s) {
+    int* w = error_word();
+    if (!w) return RC_ERR_ALLOC;
+    int v = 0;
+    if (cudaMemcpyAsync(&v, w, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return RC_ERR_CUDA;
+    return v;
 }
 
 namespace {

@@ -49,10 +49,15 @@ void* workspace(cudaStream_t stream, size_t bytes, int slot = 0);
 // Device int used as a per-call status word when the caller passes none.
 int* scratch_info(cudaStream_t stream);
 
-// The library's device error word of the current device (zero-initialised once): kernels
-// whose bounded waits run out write RC_ERR_TIMEOUT there; rc_device_status reads and
-// clears it.
+// The library's device error word of the current device (two ints, zero-initialised
+// once): kernels whose bounded waits run out write RC_ERR_TIMEOUT to the first and the
+// site of the first timeout to the second; rc_device_status reads and clears them. The
+// word is sticky: while it is set, every tensor-core kernel returns at once.
 int* error_word();
+
+// Synchronise s and return the error word's status (RC_SUCCESS when clear) without
+// clearing it; RC_ERR_CUDA / RC_ERR_ALLOC when it cannot be read.
+int pending_error(cudaStream_t s);
 
 // Wall-clock limit of every bounded device-side wait, in nanoseconds (default 2 s).
 uint64_t wait_limit_ns();

@@ -716,6 +716,7 @@ struct Mixed {
     OzakiA oz;            // digit split of A (valid when use_oz)
     void* oz_p = nullptr; // one sliced product's buffers
     bool use_oz = false;
+    int* errw = nullptr;  // the library's device error word (a timed-out wait sets it)
     View<const double> Av() const { return {A, 1, lda}; }
     View<float> Wv() const { return {W, ldw, 1}; }
 
@@ -801,7 +802,7 @@ struct Mixed {
                 const void* op2 = static_cast<const char*>(op) + (size_t)w1 * ldo * esz;
                 RC_TRY(ok(cudaStreamWaitEvent(s, ev_packed, 0)));
                 RC_TRY(gemm_tc_pair_kmajor(bf16, r2, r2, w, -1.f, op2, ldo, op2, ldo, 1.f, Wm.sub(k1 + w1, k1 + w1),
-                                           kLower, 0, s));
+                                           kLower, 0, s, info));
                 RC_TRY(ok(cudaEventRecord(ev_t2, s)));
                 t2_pending = true;
             } else {
@@ -877,10 +878,12 @@ struct Mixed {
         col_reduce_kernel<<<(unsigned)(nrhs < 1024 ? nrhs : 1024), 256, 0, s>>>(n, nrhs, U, ldu, V, ldv, mode, dst);
         RC_TRY(check_launch());
         out.resize(nrhs);
+        int e = 0;  // every host synchronisation of the refinement also reads the error word
         if (cudaMemcpyAsync(out.data(), dst, nrhs * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(&e, errw, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess)
             return RC_ERR_CUDA;
-        return RC_SUCCESS;
+        return e != 0 ? RC_ERR_TIMEOUT : RC_SUCCESS;
     }
 
     int upload(const std::vector<double>& v, double* dst) {
@@ -913,13 +916,21 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     const bool adaptive = o.shift_factor < 0.0;
     double theta = adaptive ? 0.25 * uf : o.shift_factor * uf;
 
+    // The error word is sticky: a timeout left by an earlier call (not yet read by
+    // rc_device_status) would make every tensor-core kernel of this solve return at once.
+    int* errw = error_word();
+    if (!errw) return RC_ERR_ALLOC;
+    {
+        const int e = pending_error(s);
+        if (e != RC_SUCCESS) return e;
+    }
     size_t bytes = 0;
     mixed_workspace_bytes(n, nrhs, prec, o.outer, &bytes);
     char* base = static_cast<char*>(workspace(s, bytes, 6));
     if (!base) return RC_ERR_ALLOC;
     Buf buf{base};
     Mixed M;
-    M.n = n; M.nrhs = nrhs; M.prec = prec; M.s = s; M.A = A; M.lda = lda;
+    M.n = n; M.nrhs = nrhs; M.prec = prec; M.s = s; M.A = A; M.lda = lda; M.errw = errw;
     M.ldw = (n + 31) / 32 * 32;
     M.nblk = (n + kNB - 1) / kNB;
     M.W = buf.take<float>((size_t)n * M.ldw);
@@ -950,9 +961,17 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
         rsum = buf.take<double>((size_t)((n + 127) / 128) * ((n + 127) / 128 * 128));
     }
 
-    cudaEvent_t e0, e1, e2;
-    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
-    cudaEventRecord(e0, s);
+    struct Timers {  // destroyed on every return path
+        cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+        ~Timers() {
+            for (cudaEvent_t x : e)
+                if (x) cudaEventDestroy(x);
+        }
+    } tm;
+    for (cudaEvent_t& x : tm.e)
+        if (cudaEventCreate(&x) != cudaSuccess) return RC_ERR_CUDA;
+    cudaEvent_t e0 = tm.e[0], e1 = tm.e[1], e2 = tm.e[2];
+    if (cudaEventRecord(e0, s) != cudaSuccess) return RC_ERR_CUDA;
     const View<const double> Av = M.Av();
     diag_scale_kernel<<<ceil_div(n, 256) < 1024u ? ceil_div(n, 256) : 1024u, 256, 0, s>>>(n, Av, M.sc);
     RC_TRY(check_launch());
@@ -982,13 +1001,16 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
             RC_TRY(check_launch());
         }
         RC_TRY(M.factor(o.outer, d_info));
+        int h_err = 0;
         if (cudaMemcpyAsync(&h_info, d_info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(&h_err, errw, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess)
             return RC_ERR_CUDA;
+        if (h_err != 0) return RC_ERR_TIMEOUT;  // a wait of the factorisation ran out
         if (h_info == 0 || !adaptive || attempt == 2) break;
         theta = (attempt == 0 ? 2.0 : 16.0) * uf;
     }
-    cudaEventRecord(e1, s);
+    if (cudaEventRecord(e1, s) != cudaSuccess) return RC_ERR_CUDA;
     rc_refine_info info = {};
     info.shift = theta;
     if (h_info != 0) {
@@ -1010,10 +1032,13 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     }
     double normA = 0.0;
     int split_flag = 0;
+    int h_err = 0;
     if (cudaMemcpyAsync(&normA, M.dev_scalars, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         (M.use_oz && cudaMemcpyAsync(&split_flag, M.oz.flag, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
+        cudaMemcpyAsync(&h_err, errw, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         return RC_ERR_CUDA;
+    if (h_err != 0) return RC_ERR_TIMEOUT;
     if (split_flag) M.use_oz = false;  // the diagonal did not bound A: FP64 DMMA products
     std::vector<double> normB, normX, normR, rz, pq, alpha(nrhs), beta(nrhs);
     RC_TRY(M.col_reduce(B, ldb, nullptr, 0, 0, normB, M.dev_scalars));
@@ -1105,12 +1130,14 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
         col_xpby_kernel<<<g, 256, 0, s>>>(n, nrhs, M.dev_scalars + 4 * nrhs, M.Z, ldm, M.P, ldm);
         RC_TRY(check_launch());
     }
-    cudaEventRecord(e2, s);
-    cudaEventSynchronize(e2);
+    if (cudaEventRecord(e2, s) != cudaSuccess || cudaEventSynchronize(e2) != cudaSuccess) return RC_ERR_CUDA;
+    {
+        const int e = pending_error(s);  // the last products ran after the last check
+        if (e != RC_SUCCESS) return e;
+    }
     float t_f = 0.f, t_r = 0.f;
     cudaEventElapsedTime(&t_f, e0, e1);
     cudaEventElapsedTime(&t_r, e1, e2);
-    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
     info.iterations = iters;
     info.residuals = residuals;
     info.backward_error = worst;

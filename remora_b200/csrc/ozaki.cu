@@ -209,6 +209,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     const int KB = (int)((k1 - k0 + 127) / 128);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int brows = S * nr, bbox = brows < 256 ? brows : 256;
+    if (aborted(err)) return;  // an earlier wait of the device timed out
 
     if (threadIdx.x == 0) {
         for (int q = 0; q < A_STAGES; ++q) {
@@ -240,8 +241,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             int a_issued = 0, b_issued = 0;
             for (int kb = 0; kb < KB && !*stop; ++kb) {
                 const int bs = kb & 1;
-                if (!mbar_wait_bounded(&bempty[bs], ((kb >> 1) & 1) ^ 1, stop, limit_ns)) {
-                    raise_stop(stop, err);
+                const int w = mbar_wait_bounded(&bempty[bs], ((kb >> 1) & 1) ^ 1, stop, err, nullptr, limit_ns);
+                if (w != kWaitOk) {
+                    raise_stop(stop, err, w, kSiteOzaki * 100 + kRoleProducer * 10);
                     break;
                 }
                 const int kx = (int)(k0 + 128 * kb);
@@ -250,8 +252,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 ++b_issued;
                 for (int t = 0; t < S; ++t) {
                     const int as = a_issued % A_STAGES;
-                    if (!mbar_wait_bounded(&aempty[as], ((a_issued / A_STAGES) & 1) ^ 1, stop, limit_ns)) {
-                        raise_stop(stop, err);
+                    const int wa =
+                        mbar_wait_bounded(&aempty[as], ((a_issued / A_STAGES) & 1) ^ 1, stop, err, nullptr, limit_ns);
+                    if (wa != kWaitOk) {
+                        raise_stop(stop, err, wa, kSiteOzaki * 100 + kRoleProducer * 10);
                         break;
                     }
                     mbar_expect_tx(&afull[as], (uint32_t)A_TILE);
@@ -262,10 +266,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             if (*stop) {
                 // Let the copies this thread started land before the CTA's shared memory goes away.
                 volatile int never = 0;
+                bool drained = true;
                 for (int q = (a_issued > A_STAGES ? a_issued - A_STAGES : 0); q < a_issued; ++q)
-                    mbar_wait_bounded(&afull[q % A_STAGES], (q / A_STAGES) & 1, &never, limit_ns);
+                    drained &= mbar_wait_bounded(&afull[q % A_STAGES], (q / A_STAGES) & 1, &never, nullptr, nullptr,
+                                                 limit_ns) == kWaitOk;
                 for (int q = (b_issued > 2 ? b_issued - 2 : 0); q < b_issued; ++q)
-                    mbar_wait_bounded(&bfull[q & 1], (q >> 1) & 1, &never, limit_ns);
+                    drained &= mbar_wait_bounded(&bfull[q & 1], (q >> 1) & 1, &never, nullptr, nullptr, limit_ns) ==
+                               kWaitOk;
+                if (!drained) settle(kSettleNs);
             }
         }
     } else if (warp == 1) {
@@ -273,8 +281,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             int a_used = 0;
             for (int kb = 0; kb < KB && !*stop; ++kb) {
                 const int bs = kb & 1;
-                if (!mbar_wait_bounded(&bfull[bs], (kb >> 1) & 1, stop, limit_ns)) {
-                    raise_stop(stop, err);
+                const int w = mbar_wait_bounded(&bfull[bs], (kb >> 1) & 1, stop, err, nullptr, limit_ns);
+                if (w != kWaitOk) {
+                    raise_stop(stop, err, w, kSiteOzaki * 100 + kRoleMma * 10);
                     break;
                 }
                 tc_fence_after();
@@ -282,8 +291,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 const uint64_t bd1 = sw128_kmajor_desc(sB + bs * b_bytes + 256 * 128);
                 for (int t = 0; t < S; ++t) {
                     const int as = a_used % A_STAGES;
-                    if (!mbar_wait_bounded(&afull[as], (a_used / A_STAGES) & 1, stop, limit_ns)) {
-                        raise_stop(stop, err);
+                    const int wa = mbar_wait_bounded(&afull[as], (a_used / A_STAGES) & 1, stop, err, nullptr, limit_ns);
+                    if (wa != kWaitOk) {
+                        raise_stop(stop, err, wa, kSiteOzaki * 100 + kRoleMma * 10);
                         break;
                     }
                     tc_fence_after();
@@ -307,8 +317,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         }
     } else {
         const int q = warp & 3;  // TMEM lane quadrant this warp may access
-        const bool ok = mbar_wait_bounded(done, 0, stop, limit_ns);
-        if (!ok) raise_stop(stop, err);
+        const int w = mbar_wait_bounded(done, 0, stop, err, nullptr, limit_ns);
+        const bool ok = w == kWaitOk;
+        if (!ok) raise_stop(stop, err, w, kSiteOzaki * 100 + kRoleEpilogue * 10);
         tc_fence_after();
         if (__all_sync(0xffffffffu, ok && !*stop)) {
             const int64_t i = m0 + 32 * q + lane;

@@ -9,11 +9,11 @@ namespace tc {
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
+// Bounded waits. Every spin of the tensor-core pipelines is limited by the SM's own cycle
+// counter (clock64: per SM, monotonic, unaffected by changes of the GPU's global timer),
+// 2 cycles per nanosecond of the library's wait limit, i.e. at least that wall time at any
+// SM clock up to 2 GHz.
+__device__ __forceinline__ long long wait_cycles(uint64_t limit_ns) { return (long long)(limit_ns * 2u); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
@@ -34,21 +34,51 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait on an mbarrier phase: false when limit_ns elapsed or *stop was raised.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, volatile int* stop, uint64_t limit_ns) {
-    if (mbar_try(bar, parity)) return true;
-    const uint64_t t0 = global_ns();
-    while (true) {
-        if (mbar_try(bar, parity)) return true;
-        if (*stop) return false;
-        if (global_ns() - t0 > limit_ns) return false;
+__device__ __forceinline__ bool aborted(const int* abort) { return abort != nullptr && *(volatile const int*)abort != 0; }
+
+// Outcome of a bounded wait.
+enum WaitResult { kWaitOk = 0, kWaitAborted = 1, kWaitTimeout = 2 };
+
+// Bounded wait on an mbarrier phase. kWaitAborted: this CTA's *stop was raised, or one of
+// the device-wide words err (the library's error word: a wait somewhere timed out) and
+// abort (a failed pivot of the factorisation) became non-zero -- every CTA of every
+// tensor-core kernel gives up within microseconds of the first failure instead of waiting
+// out its own limit. kWaitTimeout: the limit ran out.
+__device__ __forceinline__ int mbar_wait_bounded(uint64_t* bar, uint32_t parity, volatile int* stop, const int* err,
+                                                 const int* abort, uint64_t limit_ns) {
+    if (mbar_try(bar, parity)) return kWaitOk;
+    const long long t0 = clock64(), lim = wait_cycles(limit_ns);
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try(bar, parity)) return kWaitOk;
+        if (*stop) return kWaitAborted;
+        if ((it & 15u) == 0 && (aborted(err) || aborted(abort))) return kWaitAborted;
+        if (clock64() - t0 > lim) return kWaitTimeout;
     }
 }
 
-__device__ __forceinline__ void raise_stop(volatile int* stop, int* err) {
+// Where a wait ran out (the second int of the error word): kernel * 100 + role * 10 + the
+// CTA's rank in its cluster.
+enum WaitKernel { kSiteTcGemm = 1, kSiteTcPair = 2, kSiteOzaki = 3, kSiteSelftest = 9 };
+enum WaitRole { kRoleProducer = 0, kRoleMma = 1, kRoleEpilogue = 2, kRoleDrain = 3 };
+
+// Stop this CTA's roles; on a timeout also record RC_ERR_TIMEOUT (and, for the first one on
+// the device, its site) in the error word, which stops every other CTA's waits.
+__device__ __forceinline__ void raise_stop(volatile int* stop, int* err, int result, int site) {
     *stop = 1;
-    if (err) atomicExch(err, RC_ERR_TIMEOUT);
+    if (result == kWaitTimeout && err != nullptr) {
+        if (atomicCAS(err, 0, RC_ERR_TIMEOUT) == 0) atomicExch(err + 1, site);
+        __threadfence();
+    }
 }
+
+// After a stop, keep the CTA (and its shared memory) alive for about `ns` so that bulk copies
+// it or its pair peer issued, and that nothing waits for any more, land before the memory is
+// handed to another CTA.
+__device__ __forceinline__ void settle(uint64_t ns) {
+    const long long t0 = clock64(), lim = wait_cycles(ns);
+    while (clock64() - t0 < lim) __nanosleep(1000);
+}
+constexpr uint64_t kSettleNs = 2000000;  // 2 ms: a bulk copy of a few KB takes microseconds
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, uint64_t* bar, int x, int y) {
     asm volatile(
@@ -109,6 +139,13 @@ __device__ __forceinline__ uint32_t cluster_rank() {
 __device__ __forceinline__ void cluster_sync_all() {
     asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
+// Store v to the same shared-memory offset in CTA `rank` of the cluster (distributed shared
+// memory); ordered before the next cluster barrier's release.
+__device__ __forceinline__ void st_cluster_u32(const void* local, uint32_t rank, uint32_t v) {
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(local)), "r"(rank));
+    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(remote), "r"(v) : "memory");
+}
 // TMA load into this CTA's shared memory whose completion counts on the pair leader's
 // barrier (the same barrier offset with the peer bit cleared). No multicast.
 __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* tm, uint64_t* bar, int x, int y) {
@@ -165,8 +202,6 @@ __device__ __forceinline__ void tmem_ld16i(uint32_t taddr, int (&v)[16]) {
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __float_as_int(f[i]);
 }
-
-__device__ __forceinline__ bool aborted(const int* abort) { return abort != nullptr && *(volatile const int*)abort != 0; }
 
 __device__ __forceinline__ bool outside(Mask mask, int64_t off, int64_t m0, int64_t n0, int bm, int bn) {
     if (mask == kLower) return (m0 + bm - 1) - n0 - off < 0;

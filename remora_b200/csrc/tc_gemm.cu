@@ -12,13 +12,11 @@
 //               back to the producer through an mbarrier;
 //   warps 2..5  wait for the final commit, read the accumulator with tcgen05.ld (each warp
 //               its 32-lane quadrant of TMEM) and apply alpha/beta and the triangle mask.
-// Every mbarrier wait is bounded by a wall-clock limit; a wait that runs out sets the
-// library's device error word, stops the other roles, frees TMEM and returns.
-//
-// The FP32-accurate product (rc_gemm_f32 on large shapes) runs the same kernel on
-// operands split into TF32 high and low parts, concatenated along K:
-//   [A_hi A_hi A_lo] * [B_hi B_lo B_hi]^T = A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T,
-// which keeps about 22 bits of every product (the dropped A_lo B_lo^T term is ~2^-22).
+// Every mbarrier wait is bounded (tc_common.cuh); a wait that runs out records
+// RC_ERR_TIMEOUT in the library's device error word, stops the other roles, lets the
+// copies it issued land, frees TMEM and returns. A kernel that starts while the error word
+// or its abort word (a failed pivot) is set returns at once, and waits in flight give up
+// when either is raised, so one failure ends the whole factorisation within microseconds.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -68,7 +66,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     volatile int* stop = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int64_t m0 = (int64_t)blockIdx.y * 128, n0 = (int64_t)blockIdx.x * BN;
-    if (aborted(abort) || outside(mask, off, m0, n0, 128, BN)) return;
+    if (aborted(abort) || aborted(err) || outside(mask, off, m0, n0, 128, BN)) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
@@ -99,8 +97,9 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
             for (int kb = 0; kb < KB; ++kb) {
                 const int s = kb % STAGES;
                 const uint32_t ph = (kb / STAGES) & 1;
-                if (!mbar_wait_bounded(&empty[s], ph ^ 1, stop, limit_ns)) {
-                    raise_stop(stop, err);
+                const int w = mbar_wait_bounded(&empty[s], ph ^ 1, stop, err, abort, limit_ns);
+                if (w != kWaitOk) {
+                    raise_stop(stop, err, w, kSiteTcGemm * 100 + kRoleProducer * 10);
                     break;
                 }
                 mbar_expect_tx(&full[s], Cfg::A_BYTES + Cfg::B_BYTES);
@@ -109,10 +108,14 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
                 ++issued;
             }
             if (*stop) {
-                // Let the copies this thread started land before the CTA's shared memory goes away.
+                // Let the copies this thread started land before the CTA's shared memory goes
+                // away (every copy completes on its own barrier; no other thread waits now).
                 volatile int never = 0;
+                bool drained = true;
                 for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; ++kb)
-                    mbar_wait_bounded(&full[kb % STAGES], (kb / STAGES) & 1, &never, limit_ns);
+                    drained &= mbar_wait_bounded(&full[kb % STAGES], (kb / STAGES) & 1, &never, nullptr, nullptr,
+                                                 limit_ns) == kWaitOk;
+                if (!drained) settle(kSettleNs);
             }
         }
     } else if (warp == 1) {
@@ -123,8 +126,9 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
             for (int kb = 0; kb < KB; ++kb) {
                 const int s = kb % STAGES;
                 const uint32_t ph = (kb / STAGES) & 1;
-                if (!mbar_wait_bounded(&full[s], ph, stop, limit_ns)) {
-                    raise_stop(stop, err);
+                const int w = mbar_wait_bounded(&full[s], ph, stop, err, abort, limit_ns);
+                if (w != kWaitOk) {
+                    raise_stop(stop, err, w, kSiteTcGemm * 100 + kRoleMma * 10);
                     break;
                 }
                 tc_fence_after();
@@ -146,8 +150,9 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 #pragma unroll
             for (int j = 0; j < BN / 2; ++j) cpre[j] = (beta != 0.f && i < M && j < N) ? C(i, j) : 0.f;
         }
-        const bool ok = mbar_wait_bounded(done, 0, stop, limit_ns);
-        if (!ok) raise_stop(stop, err);
+        const int w = mbar_wait_bounded(done, 0, stop, err, abort, limit_ns);
+        const bool ok = w == kWaitOk;
+        if (!ok) raise_stop(stop, err, w, kSiteTcGemm * 100 + kRoleEpilogue * 10);
         tc_fence_after();
         // tcgen05.ld is warp-collective: the whole warp takes one decision.
         if (__all_sync(0xffffffffu, ok && !*stop)) {
@@ -217,8 +222,20 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 // commits every stage to the empty barriers of both CTAs and the final product to both
 // done barriers. Per SM and k-slice this moves 32 KB for a 128 x 256 x 32 product instead
 // of 48 KB, halving the B traffic of the single-CTA 128 x 256 tile. Two CTAs per SM
-// (3 stages each, 256 TMEM columns each). Every mbarrier wait is bounded; every thread of
-// both CTAs reaches the closing cluster barrier.
+// (3 stages each, 256 TMEM columns each).
+//
+// Failure handling. Every mbarrier wait is bounded and gives up as soon as the device error
+// word or the abort word is raised. The two CTAs may take different decisions (one sees a
+// word the other read as zero), so neither returns early after the first cluster barrier:
+// a stopped CTA still reaches the closing barrier, and before it each CTA writes its stop
+// flag into both CTAs' `any_stop`. When either stopped, both stay resident for a settle
+// period after the closing barrier, so that copies issued by either CTA (whose completion
+// counts on the leader's barrier, which nobody waits for any more) land first. Neither
+// cluster barrier can wait forever: every thread of both CTAs reaches each one after a
+// bounded number of bounded waits. TMEM allocation cannot wait forever either: at most two
+// tcgen05 CTAs (of any of this library's kernels) fit on an SM by shared memory, each
+// holding at most 256 of the 512 columns, and a CTA holding columns never waits on a CTA
+// that does not.
 constexpr int PAIR_STAGES = 3;
 constexpr int PAIR_A_BYTES = 128 * KB_BYTES, PAIR_B_BYTES = 128 * KB_BYTES;
 constexpr size_t PAIR_SMEM = (size_t)PAIR_STAGES * (PAIR_A_BYTES + PAIR_B_BYTES) + 1024 + 256;
@@ -227,7 +244,7 @@ template <bool BF16>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
     tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int64_t M,
                         int64_t N, int64_t K, float alpha, float beta, View<float> C, Mask mask, int64_t off,
-                        int* err, uint64_t limit_ns) {
+                        const int* abort, int* err, uint64_t limit_ns) {
     constexpr int KB_ELEMS = KB_BYTES / (BF16 ? 2 : 4);
     constexpr int MMAS_PER_STAGE = KB_BYTES / 32;
     extern __shared__ uint8_t smem_raw[];
@@ -239,6 +256,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
     uint64_t* done = empty + PAIR_STAGES;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     volatile int* stop = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    volatile int* any_stop = stop + 1;
 
     const uint32_t rank = cluster_rank();
     const int64_t m0 = (int64_t)blockIdx.y * 256, n0 = (int64_t)(blockIdx.x >> 1) * 256;
@@ -251,7 +269,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
             mbar_init(&empty[s], 1);
         }
         mbar_init(done, 1);
-        *stop = 0;
+        // A word already raised stops this CTA's roles before they start (no early return:
+        // the peer may have read the word as zero and waits at the cluster barriers).
+        *stop = (aborted(abort) || aborted(err)) ? 1 : 0;
+        *any_stop = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
@@ -266,34 +287,34 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     const int KB = (int)((K + KB_ELEMS - 1) / KB_ELEMS);
+    const int site = kSiteTcPair * 100 + (int)rank;
 
     if (warp == 0) {
         if (lane == 0) {
-            int issued = 0;
-            for (int kb = 0; kb < KB; ++kb) {
+            for (int kb = 0; kb < KB && !*stop; ++kb) {
                 const int s = kb % PAIR_STAGES;
                 const uint32_t ph = (kb / PAIR_STAGES) & 1;
-                if (!mbar_wait_bounded(&empty[s], ph ^ 1, stop, limit_ns)) {
-                    raise_stop(stop, err);
+                const int w = mbar_wait_bounded(&empty[s], ph ^ 1, stop, err, abort, limit_ns);
+                if (w != kWaitOk) {
+                    raise_stop(stop, err, w, site + kRoleProducer * 10);
                     break;
                 }
                 if (rank == 0) mbar_expect_tx(&full[s], 2 * (PAIR_A_BYTES + PAIR_B_BYTES));
                 tma_load_2d_pair(sA + s * PAIR_A_BYTES, &tmA, &full[s], kb * KB_ELEMS, (int)(m0 + 128 * rank));
                 tma_load_2d_pair(sB + s * PAIR_B_BYTES, &tmB, &full[s], kb * KB_ELEMS, (int)(n0 + 128 * rank));
-                ++issued;
             }
-            (void)issued;
         }
     } else if (warp == 1) {
         if (lane == 0 && rank == 0) {
             const uint32_t fmt = BF16 ? 1u : 2u;
             const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(256 >> 3) << 17) |
                                    ((uint32_t)(256 >> 4) << 24);
-            for (int kb = 0; kb < KB; ++kb) {
+            for (int kb = 0; kb < KB && !*stop; ++kb) {
                 const int s = kb % PAIR_STAGES;
                 const uint32_t ph = (kb / PAIR_STAGES) & 1;
-                if (!mbar_wait_bounded(&full[s], ph, stop, limit_ns)) {
-                    raise_stop(stop, err);
+                const int w = mbar_wait_bounded(&full[s], ph, stop, err, abort, limit_ns);
+                if (w != kWaitOk) {
+                    raise_stop(stop, err, w, site + kRoleMma * 10);
                     break;
                 }
                 tc_fence_after();
@@ -304,12 +325,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
                     umma_pair<BF16>(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
                 umma_commit_pair(&empty[s]);
             }
+            // Always committed: the done barriers of both CTAs complete once the MMAs issued
+            // so far (possibly none) are finished.
             umma_commit_pair(done);
         }
     } else {
         const int q = warp & 3;  // TMEM lane quadrant this warp may access
-        const bool ok = mbar_wait_bounded(done, 0, stop, limit_ns);
-        if (!ok) raise_stop(stop, err);
+        const int w = mbar_wait_bounded(done, 0, stop, err, abort, limit_ns);
+        const bool ok = w == kWaitOk;
+        if (!ok) raise_stop(stop, err, w, site + kRoleEpilogue * 10);
         tc_fence_after();
         if (__all_sync(0xffffffffu, ok && !*stop)) {
             const int64_t i = m0 + 128 * rank + 32 * q + lane;
@@ -348,22 +372,28 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
         }
     }
     tc_fence_before();
+    __syncthreads();  // this CTA's roles are over: *stop is final
+    if (threadIdx.x == 0 && *stop) {
+        st_cluster_u32((const void*)any_stop, 0, 1u);
+        st_cluster_u32((const void*)any_stop, 1, 1u);
+    }
     cluster_sync_all();  // the leader's MMAs read this CTA's shared memory until `done`
     if (warp == 1) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u));
     }
+    if (threadIdx.x == 0 && *any_stop) settle(kSettleNs);
 }
 
 template <bool BF16>
 int launch_tc_pair(const CUtensorMap& ta, const CUtensorMap& tb, int64_t m, int64_t n, int64_t k, float alpha,
-                   float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s) {
+                   float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s, const int* abort) {
     if (cudaFuncSetAttribute(tc_gemm_pair_kernel<BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)PAIR_SMEM) != cudaSuccess)
         return RC_ERR_CUDA;
     dim3 grid(2 * ceil_div(n, 256), ceil_div(m, 256));
     if (grid.y > 65535) return RC_ERR_NOT_SUPPORTED;
-    tc_gemm_pair_kernel<BF16><<<grid, TC_THREADS, PAIR_SMEM, s>>>(ta, tb, m, n, k, alpha, beta, C, mask, off,
+    tc_gemm_pair_kernel<BF16><<<grid, TC_THREADS, PAIR_SMEM, s>>>(ta, tb, m, n, k, alpha, beta, C, mask, off, abort,
                                                                   error_word(), wait_limit_ns());
     return check_launch();
 }
@@ -462,7 +492,8 @@ int gemm_tc_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, cons
 }
 
 int gemm_tc_pair_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, const void* A, int64_t lda,
-                        const void* B, int64_t ldb, float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s) {
+                        const void* B, int64_t ldb, float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s,
+                        const int* abort) {
     if (m <= 0 || n <= 0) return RC_SUCCESS;
     const int es = bf16 ? 2 : 4;
     if (k <= 0 || (reinterpret_cast<uintptr_t>(A) % 16) || (reinterpret_cast<uintptr_t>(B) % 16) || ((lda * es) % 16) ||
@@ -470,8 +501,8 @@ int gemm_tc_pair_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha,
         return RC_ERR_NOT_SUPPORTED;
     CUtensorMap ta, tb;
     if (!make_tmap(&ta, A, bf16, m, k, lda, 128) || !make_tmap(&tb, B, bf16, n, k, ldb, 128)) return RC_ERR_NOT_SUPPORTED;
-    return bf16 ? launch_tc_pair<true>(ta, tb, m, n, k, alpha, beta, C, mask, off, s)
-                : launch_tc_pair<false>(ta, tb, m, n, k, alpha, beta, C, mask, off, s);
+    return bf16 ? launch_tc_pair<true>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort)
+                : launch_tc_pair<false>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort);
 }
 
 int gemm_tc_fold_kmajor(int64_t m, int64_t k, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
@@ -497,7 +528,10 @@ __global__ void wait_selftest_kernel(int* err, uint64_t limit_ns) {
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
-    if (threadIdx.x == 0 && !mbar_wait_bounded(&bar, 0, &stop, limit_ns)) raise_stop(&stop, err);
+    if (threadIdx.x == 0) {
+        const int w = mbar_wait_bounded(&bar, 0, &stop, err, nullptr, limit_ns);
+        if (w != kWaitOk) raise_stop(&stop, err, w, kSiteSelftest * 100);
+    }
 }
 
 int pack_kmajor(int64_t rows, int64_t K, View<const float> X, void* dst, int64_t ldd, bool bf16, cudaStream_t s) {
@@ -591,14 +625,17 @@ int rc_selftest_wait_timeout(uint64_t limit_ns, void* stream) {
     return rc::check_launch();
 }
 
-int rc_device_status(void* stream) {
+int rc_device_error_site(void* stream, int* site) {
     if (cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) != cudaSuccess) return RC_ERR_CUDA;
     int* w = rc::error_word();
     if (!w) return RC_ERR_ALLOC;
-    int v = 0;
-    if (cudaMemcpy(&v, w, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return RC_ERR_CUDA;
-    if (v != 0 && cudaMemset(w, 0, sizeof(int)) != cudaSuccess) return RC_ERR_CUDA;
-    return v;
+    int v[2] = {0, 0};
+    if (cudaMemcpy(v, w, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return RC_ERR_CUDA;
+    if ((v[0] != 0 || v[1] != 0) && cudaMemset(w, 0, sizeof(v)) != cudaSuccess) return RC_ERR_CUDA;
+    if (site) *site = v[1];
+    return v[0];
 }
+
+int rc_device_status(void* stream) { return rc_device_error_site(stream, nullptr); }
 
 }  // extern "C"

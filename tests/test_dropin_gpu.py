@@ -23,9 +23,10 @@ def test_dropin_program(cuda):
 def test_dropin_headers_compile_without_cuda_toolkit():
     """The cuda_tag headers compile with the host compiler alone (no CUDA headers on the
     include path) when Remora's headers are available."""
-    ref = Path("/root/reference/include/remora")
-    if not ref.is_dir():
+    import oracle
+    if not oracle.reference_present():
         pytest.skip("Remora's headers are not on this machine")
+    ref = oracle.REF_INCLUDE / "remora"
     root = Path(__file__).resolve().parents[1]
     src = "#include <remora/cuda.hpp>\n#include <remora/remora.hpp>\nint main(){return 0;}\n"
     res = subprocess.run(["g++", "-std=c++14", "-fsyntax-only", "-w", f"-I{root / 'include'}", f"-I{ref.parent}",

@@ -107,3 +107,41 @@ def test_mixed_solve_block_steps_and_column_chunks(cuda, orc, n, nrhs):
     ref = np.array(B, order="F")
     assert orc.cholesky_solve(np.asfortranarray(A), ref) == 0
     assert np.linalg.norm(Xh - ref) / np.linalg.norm(ref) <= 100 * 1e3 * U64
+
+
+def _torch_spd(n: int, kappa: float, seed: int):
+    """The headline inputs on the device: A = Q diag(lambda) Q^T (Q from the QR of a seeded
+    Gaussian, lambda log-spaced 1 .. 1/kappa), exactly symmetric, column-major FP64."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    G = torch.randn((n, n), generator=g, device="cuda", dtype=torch.float64)
+    Q, _ = torch.linalg.qr(G)
+    lam = torch.logspace(0.0, -np.log10(kappa), n, device="cuda", dtype=torch.float64)
+    A = (Q * lam) @ Q.T
+    return (A + A.T) * 0.5
+
+
+def _torch_backward_error(A, X, B) -> float:
+    R = B - A @ X
+    normA = A.abs().sum(dim=0).max()
+    return float((R.abs().amax(dim=0) / (normA * X.abs().amax(dim=0) + B.abs().amax(dim=0))).max())
+
+
+def test_mixed_solve_back_to_back_n8192(cuda):
+    """Ten solves in a row at n = 8192 with 1024-column outer panels, so the look-ahead
+    stream's panel chain runs beside the CTA-pair trailing updates on every panel; the
+    device error word stays clear and every solve reaches the FP64 backward-error bar."""
+    import ctypes
+    import torch
+    from remora_b200 import _lib
+    n, nrhs = 8192, 64
+    A = _torch_spd(n, 1e2, seed=81)
+    B = torch.randn((nrhs, n), device="cuda", dtype=torch.float64).t()
+    X = torch.empty((nrhs, n), device="cuda", dtype=torch.float64).t()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for _ in range(10):
+        _, info, status = ops.spd_solve_mixed(A, B, "tf32", X=X)
+        assert status == 0, info
+        assert info["pivot"] == 0
+        assert _torch_backward_error(A, X, B) <= 1e-15
+    assert _lib.lib().rc_device_status(stream) == 0

@@ -92,6 +92,39 @@ def test_bounded_wait_times_out_and_context_survives(cuda):
     assert lib.rc_device_status(stream) == 0
 
 
+def test_timeout_is_sticky_and_stops_every_tensor_core_kernel(cuda):
+    """After a wait runs out, the device error word stays set until it is read: tcgen05
+    kernels launched meanwhile return without touching C, the mixed solve returns
+    RC_ERR_TIMEOUT instead of computing from a partial factor, and the site of the first
+    timeout (the self-test kernel: 900) is reported. Clearing the word restores both."""
+    lib = _lib.lib()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert lib.rc_device_status(stream) == 0
+    assert lib.rc_selftest_wait_timeout(20_000_000, stream) == 0
+    torch.cuda.synchronize()
+    A = torch.ones((512, 512), device="cuda")
+    C = torch.full((512, 512), 7.0, device="cuda")
+    ops.gemm(A, A, C, alpha=1.0, beta=0.0, tf32=True)
+    torch.cuda.synchronize()
+    assert torch.all(C == 7.0)  # the tcgen05 kernel returned at once
+    n = 600
+    G = torch.randn((n, n), device="cuda", dtype=torch.float64)
+    S = G @ G.T / n + torch.eye(n, device="cuda", dtype=torch.float64)
+    B = torch.randn((4, n), device="cuda", dtype=torch.float64).t()
+    _, _, status = ops.spd_solve_mixed(S, B, "tf32")
+    assert status == 5  # RC_ERR_TIMEOUT: the sticky word is seen before any work
+    site = ctypes.c_int(-1)
+    assert lib.rc_device_error_site(stream, ctypes.byref(site)) == 5
+    assert site.value == 900
+    assert lib.rc_device_status(stream) == 0
+    ops.gemm(A, A, C, alpha=1.0, beta=0.0, tf32=True)
+    torch.cuda.synchronize()
+    assert torch.all(C == 512.0)
+    _, info, status = ops.spd_solve_mixed(S, B, "tf32")
+    assert status == 0 and info["converged"] == 1
+    assert lib.rc_device_status(stream) == 0
+
+
 def _syrk_tc(prec: int, P: torch.Tensor, C: torch.Tensor, alpha: float, beta: float) -> None:
     """P is a row-major n x k view whose row stride is a multiple of 16 bytes (the TMA rule)."""
     n, k = P.shape
