@@ -216,9 +216,11 @@ def start_watchdog(seconds: float) -> None:
     import threading
 
     def fire():
+        import faulthandler
         print(json.dumps({"metric": METRIC, "error": f"watchdog: no result after {seconds:.0f} s",
                           "phase": _PHASE[0]}), flush=True)
-        print(f"[bench] watchdog fired in phase '{_PHASE[0]}'", file=sys.stderr, flush=True)
+        print(f"[bench] watchdog fired in phase '{_PHASE[0]}'; thread stacks:", file=sys.stderr, flush=True)
+        faulthandler.dump_traceback(file=sys.stderr, all_threads=True)
         os._exit(3)
 
     t = threading.Timer(seconds, fire)
@@ -281,8 +283,9 @@ def run_ours(args) -> None:
     infos = []
     with Clocks(local) as clk:
         e0.record(stream)
-        for _ in range(args.steps):
+        for i in range(args.steps):
             infos.append(step())
+            _PHASE[0] = f"timed step {i + 1} of {args.steps} done"
         e1.record(stream)
         barrier()
     launches = lib.rc_launch_count() - launches0
@@ -519,7 +522,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--case", choices=["syrk_tc", "dgemm", "potrf", "rng", "mixed", "batched", "sliced"],
                     help="run one small kernel case (for ncu captures) instead of the benchmark")
-    ap.add_argument("--watchdog", type=float, default=900.0,
+    ap.add_argument("--watchdog", type=float, default=600.0,
                     help="seconds after which a run that has not finished exits with status 3")
     args = ap.parse_args()
     if args.watchdog > 0:

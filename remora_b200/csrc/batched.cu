@@ -222,7 +222,10 @@ struct Plan {
 };
 
 std::mutex g_mutex;
-std::map<std::tuple<int, const void*, const void*, const int*, int>, std::unique_ptr<Plan>> g_plans;
+// (device, element size, A pointer array, b pointer array, info, count) -> plan. The element
+// size is part of the key: a plan's graph holds a kernel for one element type, and arrays of
+// another type can come back at the same addresses.
+std::map<std::tuple<int, int, const void*, const void*, const int*, int>, std::unique_ptr<Plan>> g_plans;
 std::map<std::pair<int, int>, Config> g_tuned;  // (sizeof(T), bucket of the largest n) -> config
 
 int size_bucket(const std::vector<int>& sizes) {
@@ -320,7 +323,7 @@ int batched(size_t count, const int* h_n, T* const* d_A, T* const* d_b, int* d_i
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return RC_ERR_CUDA;
     std::lock_guard<std::mutex> lock(g_mutex);
-    auto key = std::make_tuple(dev, (const void*)d_A, (const void*)d_b, (const int*)d_info, (int)count);
+    auto key = std::make_tuple(dev, (int)sizeof(T), (const void*)d_A, (const void*)d_b, (const int*)d_info, (int)count);
     std::unique_ptr<Plan>& slot = g_plans[key];
     std::vector<int> sizes(h_n, h_n + count);
     if (slot && slot->sizes != sizes) slot.reset();

@@ -21,6 +21,8 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <cstring>
+
 #include "assign.cuh"
 #include "gemm.cuh"
 #include "tc_gemm.cuh"
@@ -213,54 +215,98 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     }
 }
 
-// Pair kernel: a cluster of two CTAs computes one 256 x 256 tile with
+// Pair kernel: persistent clusters of two CTAs, each computing 256 x 256 tiles with
 // tcgen05.mma.cta_group::2. CTA rank r (0 = the leader) stages rows [128 r, 128 r + 128)
 // of the tile's A rows and of its B rows (K-major) in its own shared memory at the same
 // offsets, and holds the accumulator of its 128 rows (x 256 columns) in its own TMEM.
 // Both CTAs issue their TMA loads against the leader's full barrier (peer bit cleared),
 // whose expected byte count covers both; one thread of the leader issues the MMAs and
-// commits every stage to the empty barriers of both CTAs and the final product to both
-// done barriers. Per SM and k-slice this moves 32 KB for a 128 x 256 x 32 product instead
-// of 48 KB, halving the B traffic of the single-CTA 128 x 256 tile. Two CTAs per SM
-// (3 stages each, 256 TMEM columns each).
+// commits every stage to the empty barriers of both CTAs and every finished tile to both
+// tfull barriers. Per SM and k-slice this moves 32 KB for a 128 x 256 x 32 product instead
+// of 48 KB, half the B traffic of a single-CTA 128 x 256 tile.
 //
-// Failure handling. Every mbarrier wait is bounded and gives up as soon as the device error
-// word or the abort word is raised. The two CTAs may take different decisions (one sees a
-// word the other read as zero), so neither returns early after the first cluster barrier:
-// a stopped CTA still reaches the closing barrier, and before it each CTA writes its stop
-// flag into both CTAs' `any_stop`. When either stopped, both stay resident for a settle
-// period after the closing barrier, so that copies issued by either CTA (whose completion
-// counts on the leader's barrier, which nobody waits for any more) land first. Neither
-// cluster barrier can wait forever: every thread of both CTAs reaches each one after a
-// bounded number of bounded waits. TMEM allocation cannot wait forever either: at most two
-// tcgen05 CTAs (of any of this library's kernels) fit on an SM by shared memory, each
-// holding at most 256 of the 512 columns, and a CTA holding columns never waits on a CTA
-// that does not.
+// Persistence. Cluster c takes tiles c, c + C, c + 2C, ... of a fixed enumeration (all
+// tiles, or the tiles on and below the diagonal of a square C). The loads of the next tile
+// stream into the ring while the epilogue still drains the accumulator; the leader's MMAs
+// of the next tile wait on its tempty barrier, which both CTAs' epilogue groups arrive on
+// once their TMEM reads are done.
+//
+// Epilogue. Fast path (beta = 1, C row-major and 16-byte aligned, tile off the diagonal):
+// each epilogue warp moves its 32 rows 16 columns at a time TMEM -> registers (x alpha) ->
+// a 64-byte-swizzled staging box in shared memory -> a TMA reduce-add into C, with two
+// staging boxes per warp in flight; C is never read by the SM. Otherwise the rows are
+// finished element by element (the triangle mask, general beta).
+//
+// One CTA per SM. The shared-memory footprint is at least half an SM's, so no SM holds two
+// pair CTAs and no TPC holds two pairs. (Two pairs on one TPC can allocate TMEM in crossed
+// order -- each pair holding on one SM the columns the other pair waits for on the other
+// SM -- and then both wait forever.) A single-CTA tcgen05 kernel (at most 256 columns, it
+// waits on no other CTA) may run beside a pair CTA; the pair's collective allocation then
+// waits at most until that CTA finishes.
+//
+// Failure handling. Every mbarrier wait is bounded and gives up as soon as the device
+// error word or the abort word is raised; the epilogue warps take each decision together
+// (a barrier-reduction over their 128 threads). The two CTAs may still take different
+// decisions, so neither returns early: each reaches the closing cluster barrier, having
+// written its stop flag into both CTAs' `any_stop`; when either stopped, both stay
+// resident for a settle period so that copies still in flight land first.
 constexpr int PAIR_STAGES = 3;
 constexpr int PAIR_A_BYTES = 128 * KB_BYTES, PAIR_B_BYTES = 128 * KB_BYTES;
-constexpr size_t PAIR_SMEM = (size_t)PAIR_STAGES * (PAIR_A_BYTES + PAIR_B_BYTES) + 1024 + 256;
+constexpr int EPI_COLS = 16;                        // columns of one staged box (64 bytes of FP32)
+constexpr int EPI_BOX_BYTES = 32 * EPI_COLS * 4;    // 32 rows x 16 columns: 2 KB
+constexpr int EPI_BUFS = 2;                         // staged boxes in flight per warp
+constexpr int PAIR_STAGING_BYTES = 4 * EPI_BUFS * EPI_BOX_BYTES;
+constexpr size_t PAIR_SMEM_BASE =
+    1024 + (size_t)PAIR_STAGES * (PAIR_A_BYTES + PAIR_B_BYTES) + PAIR_STAGING_BYTES + 256;
+
+// The tile enumeration of one pair launch: mode 0 all tm_count x tn_count tiles (row by
+// row), mode 1 the tiles (tm, tn) with tn <= tm of a square grid, mode 2 those with tn >= tm.
+struct PairTiles {
+    int mode;
+    int64_t tm_count, tn_count, total;
+};
+
+__device__ __forceinline__ void pair_tile(const PairTiles& pt, int64_t t, int64_t& tm, int64_t& tn) {
+    if (pt.mode == 0) {
+        tm = t / pt.tn_count;
+        tn = t % pt.tn_count;
+        return;
+    }
+    int64_t r = (int64_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((r + 1) * (r + 2) / 2 <= t) ++r;
+    while (r * (r + 1) / 2 > t) --r;
+    tm = r;
+    tn = t - r * (r + 1) / 2;
+    if (pt.mode == 2) {
+        const int64_t x = tm;
+        tm = tn;
+        tn = x;
+    }
+}
 
 template <bool BF16>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
-    tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int64_t M,
-                        int64_t N, int64_t K, float alpha, float beta, View<float> C, Mask mask, int64_t off,
-                        const int* abort, int* err, uint64_t limit_ns) {
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
+    tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                        const __grid_constant__ CUtensorMap tmC, int64_t M, int64_t N, int64_t K, float alpha,
+                        float beta, View<float> C, Mask mask, PairTiles pt, int fast, const int* abort, int* err,
+                        uint64_t limit_ns) {
     constexpr int KB_ELEMS = KB_BYTES / (BF16 ? 2 : 4);
     constexpr int MMAS_PER_STAGE = KB_BYTES / 32;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;
-    uint8_t* sB = smem + PAIR_STAGES * PAIR_A_BYTES;
-    uint64_t* full = reinterpret_cast<uint64_t*>(sB + PAIR_STAGES * PAIR_B_BYTES);
+    uint8_t* sB = sA + PAIR_STAGES * PAIR_A_BYTES;
+    uint8_t* stage_c = sB + PAIR_STAGES * PAIR_B_BYTES;  // 4 warps x EPI_BUFS boxes, 2 KB each
+    uint64_t* full = reinterpret_cast<uint64_t*>(stage_c + PAIR_STAGING_BYTES);
     uint64_t* empty = full + PAIR_STAGES;
-    uint64_t* done = empty + PAIR_STAGES;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* tfull = empty + PAIR_STAGES;
+    uint64_t* tempty = tfull + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
     volatile int* stop = reinterpret_cast<volatile int*>(tmem_slot + 1);
     volatile int* any_stop = stop + 1;
 
     const uint32_t rank = cluster_rank();
-    const int64_t m0 = (int64_t)blockIdx.y * 256, n0 = (int64_t)(blockIdx.x >> 1) * 256;
-    if (outside(mask, off, m0, n0, 256, 256)) return;  // the same decision in both CTAs
+    const int64_t cluster = blockIdx.x >> 1, nclusters = gridDim.x >> 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
@@ -268,7 +314,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(done, 1);
+        mbar_init(tfull, 1);
+        mbar_init(tempty, 2);  // one arrival per CTA's epilogue group (used in the leader)
         // A word already raised stops this CTA's roles before they start (no early return:
         // the peer may have read the word as zero and waits at the cluster barriers).
         *stop = (aborted(abort) || aborted(err)) ? 1 : 0;
@@ -276,6 +323,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
+        if (fast) asm volatile("prefetch.tensormap [%0];" ::"l"(&tmC) : "memory");
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -291,17 +339,23 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
 
     if (warp == 0) {
         if (lane == 0) {
-            for (int kb = 0; kb < KB && !*stop; ++kb) {
-                const int s = kb % PAIR_STAGES;
-                const uint32_t ph = (kb / PAIR_STAGES) & 1;
-                const int w = mbar_wait_bounded(&empty[s], ph ^ 1, stop, err, abort, limit_ns);
-                if (w != kWaitOk) {
-                    raise_stop(stop, err, w, site + kRoleProducer * 10);
-                    break;
+            int64_t g = 0;  // k-blocks issued so far, over all tiles of this cluster
+            for (int64_t t = cluster; t < pt.total && !*stop; t += nclusters) {
+                int64_t tm, tn;
+                pair_tile(pt, t, tm, tn);
+                const int am = (int)(tm * 256 + 128 * rank), bn = (int)(tn * 256 + 128 * rank);
+                for (int kb = 0; kb < KB; ++kb, ++g) {
+                    const int s = (int)(g % PAIR_STAGES);
+                    const uint32_t ph = (uint32_t)((g / PAIR_STAGES) & 1);
+                    const int w = mbar_wait_bounded(&empty[s], ph ^ 1, stop, err, abort, limit_ns);
+                    if (w != kWaitOk) {
+                        raise_stop(stop, err, w, site + kRoleProducer * 10);
+                        break;
+                    }
+                    if (rank == 0) mbar_expect_tx(&full[s], 2 * (PAIR_A_BYTES + PAIR_B_BYTES));
+                    tma_load_2d_pair(sA + s * PAIR_A_BYTES, &tmA, &full[s], kb * KB_ELEMS, am);
+                    tma_load_2d_pair(sB + s * PAIR_B_BYTES, &tmB, &full[s], kb * KB_ELEMS, bn);
                 }
-                if (rank == 0) mbar_expect_tx(&full[s], 2 * (PAIR_A_BYTES + PAIR_B_BYTES));
-                tma_load_2d_pair(sA + s * PAIR_A_BYTES, &tmA, &full[s], kb * KB_ELEMS, (int)(m0 + 128 * rank));
-                tma_load_2d_pair(sB + s * PAIR_B_BYTES, &tmB, &full[s], kb * KB_ELEMS, (int)(n0 + 128 * rank));
             }
         }
     } else if (warp == 1) {
@@ -309,67 +363,123 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
             const uint32_t fmt = BF16 ? 1u : 2u;
             const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(256 >> 3) << 17) |
                                    ((uint32_t)(256 >> 4) << 24);
-            for (int kb = 0; kb < KB && !*stop; ++kb) {
-                const int s = kb % PAIR_STAGES;
-                const uint32_t ph = (kb / PAIR_STAGES) & 1;
-                const int w = mbar_wait_bounded(&full[s], ph, stop, err, abort, limit_ns);
-                if (w != kWaitOk) {
-                    raise_stop(stop, err, w, site + kRoleMma * 10);
-                    break;
+            int64_t g = 0;
+            int it = 0;
+            for (int64_t t = cluster; t < pt.total && !*stop; t += nclusters, ++it) {
+                if (it > 0) {  // both epilogue groups have read the previous tile's accumulator
+                    const int w = mbar_wait_bounded(tempty, (uint32_t)((it - 1) & 1), stop, err, abort, limit_ns);
+                    if (w != kWaitOk) {
+                        raise_stop(stop, err, w, site + kRoleMma * 10);
+                        break;
+                    }
+                    tc_fence_after();
                 }
-                tc_fence_after();
-                const uint64_t ad = sw128_kmajor_desc(sA + s * PAIR_A_BYTES);
-                const uint64_t bd = sw128_kmajor_desc(sB + s * PAIR_B_BYTES);
+                for (int kb = 0; kb < KB; ++kb, ++g) {
+                    const int s = (int)(g % PAIR_STAGES);
+                    const uint32_t ph = (uint32_t)((g / PAIR_STAGES) & 1);
+                    const int w = mbar_wait_bounded(&full[s], ph, stop, err, abort, limit_ns);
+                    if (w != kWaitOk) {
+                        raise_stop(stop, err, w, site + kRoleMma * 10);
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t ad = sw128_kmajor_desc(sA + s * PAIR_A_BYTES);
+                    const uint64_t bd = sw128_kmajor_desc(sB + s * PAIR_B_BYTES);
 #pragma unroll
-                for (int kk = 0; kk < MMAS_PER_STAGE; ++kk)
-                    umma_pair<BF16>(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
-                umma_commit_pair(&empty[s]);
+                    for (int kk = 0; kk < MMAS_PER_STAGE; ++kk)
+                        umma_pair<BF16>(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
+                    umma_commit_pair(&empty[s]);
+                }
+                // The tile's accumulator is complete once the MMAs issued so far finish (on a
+                // stop: whatever was issued; the epilogue then skips the tile).
+                umma_commit_pair(tfull);
             }
-            // Always committed: the done barriers of both CTAs complete once the MMAs issued
-            // so far (possibly none) are finished.
-            umma_commit_pair(done);
         }
     } else {
         const int q = warp & 3;  // TMEM lane quadrant this warp may access
-        const int w = mbar_wait_bounded(done, 0, stop, err, abort, limit_ns);
-        const bool ok = w == kWaitOk;
-        if (!ok) raise_stop(stop, err, w, site + kRoleEpilogue * 10);
-        tc_fence_after();
-        if (__all_sync(0xffffffffu, ok && !*stop)) {
-            const int64_t i = m0 + 128 * rank + 32 * q + lane;
-            const bool row_ok = i < M;
-            const bool vec = C.cs == 1 && (C.rs % 4 == 0) && (reinterpret_cast<uintptr_t>(C.p) % 16 == 0);
+        uint8_t* my_stage = stage_c + q * EPI_BUFS * EPI_BOX_BYTES;
+        const bool vec = C.cs == 1 && (C.rs % 4 == 0) && (reinterpret_cast<uintptr_t>(C.p) % 16 == 0);
+        int it = 0, issued = 0;
+        for (int64_t t = cluster; t < pt.total; t += nclusters, ++it) {
+            const int w = mbar_wait_bounded(tfull, (uint32_t)(it & 1), stop, err, abort, limit_ns);
+            // One decision for the four epilogue warps (their barrier below counts all 128).
+            if (epilogue_any(w != kWaitOk || *stop, 128)) {
+                if (w != kWaitOk) raise_stop(stop, err, w, site + kRoleEpilogue * 10);
+                else *stop = 1;
+                break;
+            }
+            tc_fence_after();
+            int64_t tm, tn;
+            pair_tile(pt, t, tm, tn);
+            const int64_t m0 = tm * 256, n0 = tn * 256;
+            const int64_t r0 = m0 + 128 * rank + 32 * q;  // this warp's first row
+            const int64_t i = r0 + lane;
+            const bool diag = mask != kFull && tm == tn;
+            if (fast && !diag) {
 #pragma unroll 1
-            for (int c0 = 0; c0 < 256; c0 += 16) {
-                float v[16];
-                tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
-                if (!row_ok) continue;
-                const int64_t j0 = n0 + c0;
-                if (vec && j0 + 15 < N && keep(mask, off, i, j0 + 15) && keep(mask, off, i, j0)) {
-                    float4* dst = reinterpret_cast<float4*>(C.p + i * C.rs + j0);
+                for (int c0 = 0; c0 < 256; c0 += EPI_COLS) {
+                    float v[16];
+                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+                    uint8_t* box = my_stage + (issued & (EPI_BUFS - 1)) * EPI_BOX_BYTES;
+                    if (issued >= EPI_BUFS) {  // the box written two steps ago has been read
+                        if (lane == 0) bulk_wait_read_1();
+                        __syncwarp();
+                    }
+                    // row `lane` of the box: 64 bytes, 16-byte chunks swizzled by (row / 2) mod 4
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
-                        float4 r = make_float4(alpha * v[4 * u], alpha * v[4 * u + 1], alpha * v[4 * u + 2],
-                                               alpha * v[4 * u + 3]);
-                        if (beta != 0.f) {
-                            const float4 c = dst[u];
-                            r.x = fmaf(beta, c.x, r.x); r.y = fmaf(beta, c.y, r.y);
-                            r.z = fmaf(beta, c.z, r.z); r.w = fmaf(beta, c.w, r.w);
-                        }
-                        dst[u] = r;
+                        const int chunk = u ^ ((lane >> 1) & 3);
+                        *reinterpret_cast<float4*>(box + lane * 64 + chunk * 16) =
+                            make_float4(alpha * v[4 * u], alpha * v[4 * u + 1], alpha * v[4 * u + 2],
+                                        alpha * v[4 * u + 3]);
                     }
-                } else {
+                    fence_proxy_async_smem();
+                    __syncwarp();
+                    if (lane == 0) {
+                        tma_reduce_add_2d(&tmC, box, (int)(n0 + c0), (int)r0);
+                        bulk_commit();
+                    }
+                    ++issued;
+                }
+            } else {
+                const bool row_ok = i < M;
+#pragma unroll 1
+                for (int c0 = 0; c0 < 256; c0 += 16) {
+                    float v[16];
+                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+                    if (!row_ok) continue;
+                    const int64_t j0 = n0 + c0;
+                    if (vec && j0 + 15 < N && keep(mask, 0, i, j0 + 15) && keep(mask, 0, i, j0)) {
+                        float4* dst = reinterpret_cast<float4*>(C.p + i * C.rs + j0);
 #pragma unroll
-                    for (int u = 0; u < 16; ++u) {
-                        const int64_t j = j0 + u;
-                        if (j >= N || !keep(mask, off, i, j)) continue;
-                        float r = alpha * v[u];
-                        if (beta != 0.f) r = fmaf(beta, C(i, j), r);
-                        C(i, j) = r;
+                        for (int u = 0; u < 4; ++u) {
+                            float4 r = make_float4(alpha * v[4 * u], alpha * v[4 * u + 1], alpha * v[4 * u + 2],
+                                                   alpha * v[4 * u + 3]);
+                            if (beta != 0.f) {
+                                const float4 c = dst[u];
+                                r.x = fmaf(beta, c.x, r.x); r.y = fmaf(beta, c.y, r.y);
+                                r.z = fmaf(beta, c.z, r.z); r.w = fmaf(beta, c.w, r.w);
+                            }
+                            dst[u] = r;
+                        }
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) {
+                            const int64_t j = j0 + u;
+                            if (j >= N || !keep(mask, 0, i, j)) continue;
+                            float r = alpha * v[u];
+                            if (beta != 0.f) r = fmaf(beta, C(i, j), r);
+                            C(i, j) = r;
+                        }
                     }
                 }
             }
+            // This CTA's reads of the accumulator are done: release it to the leader's MMAs.
+            tc_fence_before();
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (warp == 2 && lane == 0) mbar_arrive_cluster(tempty, 0);
         }
+        if (lane == 0) bulk_wait_all();  // every reduce-add of this warp has landed
     }
     tc_fence_before();
     __syncthreads();  // this CTA's roles are over: *stop is final
@@ -377,25 +487,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 2)
         st_cluster_u32((const void*)any_stop, 0, 1u);
         st_cluster_u32((const void*)any_stop, 1, 1u);
     }
-    cluster_sync_all();  // the leader's MMAs read this CTA's shared memory until `done`
+    __syncwarp();
+    cluster_sync_all();  // the leader's MMAs read this CTA's shared memory until its last tfull
     if (warp == 1) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u));
     }
     if (threadIdx.x == 0 && *any_stop) settle(kSettleNs);
-}
-
-template <bool BF16>
-int launch_tc_pair(const CUtensorMap& ta, const CUtensorMap& tb, int64_t m, int64_t n, int64_t k, float alpha,
-                   float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s, const int* abort) {
-    if (cudaFuncSetAttribute(tc_gemm_pair_kernel<BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)PAIR_SMEM) != cudaSuccess)
-        return RC_ERR_CUDA;
-    dim3 grid(2 * ceil_div(n, 256), ceil_div(m, 256));
-    if (grid.y > 65535) return RC_ERR_NOT_SUPPORTED;
-    tc_gemm_pair_kernel<BF16><<<grid, TC_THREADS, PAIR_SMEM, s>>>(ta, tb, m, n, k, alpha, beta, C, mask, off, abort,
-                                                                  error_word(), wait_limit_ns());
-    return check_launch();
 }
 
 // Split x into TF32 high part (low 13 mantissa bits cleared) and the FP32 remainder,
@@ -452,6 +550,69 @@ bool make_tmap(CUtensorMap* tm, const void* base, bool bf16, int64_t rows, int64
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tensor map of a row-major FP32 C (rows x cols, row stride ld) for the pair epilogue's
+// reduce-adds: 32-row x 16-column boxes, 64-byte swizzle (the staging layout).
+bool make_c_tmap(CUtensorMap* tm, const float* base, int64_t rows, int64_t cols, int64_t ld) {
+    auto enc = encoder();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+    cuuint32_t box[2] = {(cuuint32_t)EPI_COLS, 32u};
+    cuuint32_t estr[2] = {1, 1};
+    return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Dynamic shared memory of a pair CTA: the ring, the staging boxes and the barriers, and at
+// least half of an SM's shared memory so that no SM ever holds two pair CTAs.
+size_t pair_smem_bytes() {
+    static size_t bytes[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (!bytes[dev]) {
+        int per_sm = 0, reserved = 0;
+        if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess)
+            return 0;
+        const size_t half = (size_t)per_sm / 2 + 16 - (size_t)reserved;  // two such CTAs do not fit
+        bytes[dev] = PAIR_SMEM_BASE > half ? PAIR_SMEM_BASE : (half + 127) / 128 * 128;
+    }
+    return bytes[dev];
+}
+
+template <bool BF16>
+int launch_tc_pair(const CUtensorMap& ta, const CUtensorMap& tb, int64_t m, int64_t n, int64_t k, float alpha,
+                   float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s, const int* abort,
+                   int reserve_sms) {
+    PairTiles pt;
+    pt.tm_count = (m + 255) / 256;
+    pt.tn_count = (n + 255) / 256;
+    if (mask == kFull) {
+        pt.mode = 0;
+        pt.total = pt.tm_count * pt.tn_count;
+    } else if (off == 0 && m == n) {
+        pt.mode = mask == kLower ? 1 : 2;
+        pt.total = pt.tm_count * (pt.tm_count + 1) / 2;
+    } else {
+        return RC_ERR_NOT_SUPPORTED;
+    }
+    CUtensorMap tc;
+    std::memset(&tc, 0, sizeof(tc));
+    const bool fast = beta == 1.f && C.cs == 1 && C.rs % 4 == 0 && reinterpret_cast<uintptr_t>(C.p) % 16 == 0 &&
+                      make_c_tmap(&tc, C.p, m, n, C.rs);
+    const size_t smem = pair_smem_bytes();
+    if (smem == 0 || smem > 232448) return RC_ERR_NOT_SUPPORTED;
+    if (cudaFuncSetAttribute(tc_gemm_pair_kernel<BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return RC_ERR_CUDA;
+    const int64_t avail = (int64_t)(sm_count() - (reserve_sms > 0 ? reserve_sms : 0)) / 2;
+    const int64_t clusters = pt.total < (avail > 0 ? avail : 1) ? pt.total : (avail > 0 ? avail : 1);
+    tc_gemm_pair_kernel<BF16><<<(unsigned)(2 * clusters), TC_THREADS, smem, s>>>(
+        ta, tb, tc, m, n, k, alpha, beta, C, mask, pt, fast ? 1 : 0, abort, error_word(), wait_limit_ns());
+    return check_launch();
+}
+
 template <int BN, bool BF16, bool FOLD = false>
 int launch_tc(const CUtensorMap& ta, const CUtensorMap& tb, int64_t m, int64_t n, int64_t k, float alpha, float beta,
               View<float> C, Mask mask, int64_t off, cudaStream_t s, const int* abort) {
@@ -493,7 +654,7 @@ int gemm_tc_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, cons
 
 int gemm_tc_pair_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, const void* A, int64_t lda,
                         const void* B, int64_t ldb, float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s,
-                        const int* abort) {
+                        const int* abort, int reserve_sms) {
     if (m <= 0 || n <= 0) return RC_SUCCESS;
     const int es = bf16 ? 2 : 4;
     if (k <= 0 || (reinterpret_cast<uintptr_t>(A) % 16) || (reinterpret_cast<uintptr_t>(B) % 16) || ((lda * es) % 16) ||
@@ -501,8 +662,8 @@ int gemm_tc_pair_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha,
         return RC_ERR_NOT_SUPPORTED;
     CUtensorMap ta, tb;
     if (!make_tmap(&ta, A, bf16, m, k, lda, 128) || !make_tmap(&tb, B, bf16, n, k, ldb, 128)) return RC_ERR_NOT_SUPPORTED;
-    return bf16 ? launch_tc_pair<true>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort)
-                : launch_tc_pair<false>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort);
+    return bf16 ? launch_tc_pair<true>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort, reserve_sms)
+                : launch_tc_pair<false>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort, reserve_sms);
 }
 
 int gemm_tc_fold_kmajor(int64_t m, int64_t k, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,

@@ -78,3 +78,22 @@ def test_batched_rejects_oversize(cuda):
     sys = ops.BatchedSystems(mats, rhs)
     with pytest.raises(Exception):
         sys.solve()
+
+
+def test_batched_plans_keep_element_types_apart(cuda):
+    """An FP64 batch and then an FP32 batch passed through the SAME pointer-array, info
+    buffers and sizes: the cached FP64 plan must not be replayed on FP32 storage."""
+    mats, rhs = rbf_systems(24, seed=12, lo=16, hi=200)
+    s64 = ops.BatchedSystems(mats, rhs, dtype=torch.float64)
+    s64.solve(autotune=False)
+    s32 = ops.BatchedSystems(mats, rhs, dtype=torch.float32)
+    s64.a_ptrs.copy_(s32.a_ptrs)
+    s64.b_ptrs.copy_(s32.b_ptrs)
+    s32.a_ptrs, s32.b_ptrs, s32.info = s64.a_ptrs, s64.b_ptrs, s64.info
+    s32.info.zero_()
+    s32.solve(autotune=False)
+    torch.cuda.synchronize()
+    assert torch.all(s32.info == 0)
+    for i in range(len(mats)):
+        x = s32.solution(i).double().cpu().numpy()
+        assert bwd(mats[i], x, rhs[i]) <= 1e-5, i
