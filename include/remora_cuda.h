@@ -40,6 +40,10 @@ int rc_version(void);
 const char* rc_error_string(int status);
 /* Number of kernels the library has launched so far in this process (all devices). */
 unsigned long long rc_launch_count(void);
+/* Number of device allocations the library has made for its own use so far in this
+ * process (workspaces, the error word, batched plans; not rc_malloc on a caller's behalf).
+ * No reference counterpart: it lets a host check that a call allocated nothing. */
+unsigned long long rc_allocation_count(void);
 /* Free every cached workspace of the current device (synchronises the device). */
 int rc_release_workspaces(void);
 /* Failure detection. Every device-side wait (the mbarrier phases of the tensor-core

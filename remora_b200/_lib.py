@@ -38,6 +38,7 @@ SIGNATURES: dict[str, list] = {
     "rc_error_string": [_I],
     "rc_release_workspaces": [],
     "rc_launch_count": [],
+    "rc_allocation_count": [],
     "rc_device_count": [_P],
     "rc_set_device": [_I],
     "rc_get_device": [_P],
@@ -98,7 +99,8 @@ SIGNATURES: dict[str, list] = {
     "rc_fill_f64": [_Z, _Z, c_double, _P, _Z, _P],
     "rc_fill_f32": [_Z, _Z, c_float, _P, _Z, _P],
 }
-_RESTYPES = {"rc_error_string": ctypes.c_char_p, "rc_launch_count": ctypes.c_ulonglong}
+_RESTYPES = {"rc_error_string": ctypes.c_char_p, "rc_launch_count": ctypes.c_ulonglong,
+             "rc_allocation_count": ctypes.c_ulonglong}
 
 _lib = None
 

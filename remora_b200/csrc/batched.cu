@@ -270,6 +270,7 @@ int autotune(Plan& p, cudaStream_t s) {
     for (int i = 0; i < p.count; ++i) total += (size_t)p.sizes[i] * p.sizes[i] + p.sizes[i];
     T* save = nullptr;
     if (cudaMalloc(&save, total * sizeof(T)) != cudaSuccess) return RC_ERR_ALLOC;
+    note_allocation();
     auto copy_all = [&](bool to_save) {
         size_t off = 0;
         for (int i = 0; i < p.count; ++i) {
@@ -342,6 +343,7 @@ int batched(size_t count, const int* h_n, T* const* d_A, T* const* d_b, int* d_i
         std::copy(order.begin(), order.end(), host.begin() + 1);
         std::copy(sizes.begin(), sizes.end(), host.begin() + 1 + count);
         if (cudaMalloc(&p->d_buf, host.size() * sizeof(int)) != cudaSuccess) return RC_ERR_ALLOC;
+        note_allocation();
         if (cudaMemcpy(p->d_buf, host.data(), host.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
             return RC_ERR_CUDA;
         if (autotune_flag) RC_TRY(autotune<T>(*p, s));

@@ -16,8 +16,11 @@ struct Buffer {
 std::mutex g_mutex;
 // (device, stream, slot) -> buffer
 std::map<std::tuple<int, cudaStream_t, int>, Buffer> g_buffers;
+std::atomic<unsigned long long> g_allocations{0};
 
 }  // namespace
+
+void note_allocation() { g_allocations.fetch_add(1, std::memory_order_relaxed); }
 
 int sm_count() {
     static int counts[64] = {0};
@@ -51,6 +54,7 @@ void* workspace(cudaStream_t stream, size_t bytes, int slot) {
         b.ptr = nullptr;
         return nullptr;
     }
+    note_allocation();
     b.bytes = rounded;
     return b.ptr;
 }
@@ -71,6 +75,8 @@ int* error_word() {
         if (cudaMalloc(&w, 2 * sizeof(int)) != cudaSuccess || cudaMemset(w, 0, 2 * sizeof(int)) != cudaSuccess) {
             cudaGetLastError();
             w = nullptr;
+        } else {
+            note_allocation();
         }
     }
     return w;
@@ -101,6 +107,8 @@ extern "C" {
 int rc_version(void) { return 100; }
 
 unsigned long long rc_launch_count(void) { return rc::g_launches.load(std::memory_order_relaxed); }
+
+unsigned long long rc_allocation_count(void) { return rc::g_allocations.load(std::memory_order_relaxed); }
 
 int rc_set_wait_limit_ns(uint64_t ns) {
     if (ns == 0) return RC_ERR_INVALID_ARGUMENT;

@@ -38,6 +38,9 @@ inline int check_launch() {
         if (rc_status_ != RC_SUCCESS) return rc_status_; \
     } while (0)
 
+// Count one device allocation made by the library for its own use (rc_allocation_count).
+void note_allocation();
+
 // Number of SMs of the current device (cached per device).
 int sm_count();
 

@@ -4,9 +4,11 @@ cudaMalloc's device-wide synchronisation is not allowed where they call it).
 
 Two calls in a row through the C-ABI, each compared with the allocating entry point
 rc_spd_solve_f64 on the same inputs, within the FP64 parity bar (relative Frobenius
-<= 1e-13); sizes beyond the fixed scratch must be rejected. This file sorts last so a run
-that stops at the first failure has run every other test already; it also passes alone
-in a fresh process."""
+<= 1e-13); neither call may add to the library's count of its own device allocations, and
+the second leaves the device's free memory unchanged (the first may load the module that
+holds the fixed scratch); sizes beyond the fixed scratch must be rejected. This file sorts
+last so a run that stops at the first failure has run every other test already; it also
+passes alone in a fresh process."""
 from __future__ import annotations
 
 import ctypes
@@ -32,14 +34,27 @@ def _solve(name: str, A: torch.Tensor, B: torch.Tensor) -> tuple[int, int, np.nd
 
 
 def test_no_alloc_solve_matches_allocating_solve(cuda, orc):
+    lib = _lib.lib()
     for call, (n, nrhs) in enumerate([(1024, 16), (700, 64)]):
         g = orc.rng(100 + call)
         G = g.normal(n, n)
         A = G @ G.T / n + 1e-2 * np.eye(n)
         B = g.normal(n, nrhs)
         Ad, Bd = to_dev(A, False), to_dev(B, False)
-        status, info, X_static = _solve("rc_spd_solve_f64_noalloc", Ad, Bd)
-        assert status == 0 and info == 0
+        info_d = torch.zeros(1, dtype=torch.int32, device="cuda")
+        X = Bd.clone()
+        torch.cuda.synchronize()
+        count0, free0 = lib.rc_allocation_count(), torch.cuda.mem_get_info()[0]
+        status = lib.rc_spd_solve_f64_noalloc(n, nrhs, ctypes.c_void_p(Ad.data_ptr()), Ad.stride(1),
+                                              ctypes.c_void_p(X.data_ptr()), X.stride(1),
+                                              ctypes.c_void_p(info_d.data_ptr()),
+                                              ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        assert lib.rc_allocation_count() == count0
+        if call > 0:
+            assert torch.cuda.mem_get_info()[0] == free0
+        assert status == 0 and int(info_d.item()) == 0
+        X_static = to_host(X)
         status, info, X_alloc = _solve("rc_spd_solve_f64", Ad, Bd)
         assert status == 0 and info == 0
         assert oracle.rel_fro(X_static, X_alloc) <= 1e-13
