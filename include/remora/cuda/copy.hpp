@@ -1,16 +1,81 @@
 // remora/cuda/copy.hpp -- host <-> device transport for the cuda_tag device:
 // copy_to_device(cpu expression, cuda_tag()) and copy_to_cpu(cuda expression), the
 // interface of include/remora/device_copy.hpp:33-64 and hip/copy.hpp:468-505.
-// Pitched copies (rc_memcpy2d) replace the reference's mapped host memory plus an
-// assign kernel over PCIe (hip/copy.hpp:277-294); an orientation change is a transposing
-// copy on the device. Both directions synchronise the stream before returning.
+//
+// The reference page-locks the user's host memory and lets a kernel read or write it
+// over the bus (hip/copy.hpp:131-410). Here a matrix moves in chunks of whole storage
+// lines (rows of a row-major target, columns of a column-major one) through two
+// page-locked staging chunks per (device, host thread): host threads evaluate the host
+// expression straight into one chunk (or unpack it into the host target) while the DMA of
+// the other chunk runs, so every element is touched once on the host and the copy engine
+// moves page-locked memory at the link's rate. The device side is one dense staging
+// matrix in the target's orientation; an orientation change or a strided target is a
+// device-side assignment. Both directions synchronise the stream before returning, as the
+// reference does.
 #ifndef REMORA_CUDA_COPY_HPP
 #define REMORA_CUDA_COPY_HPP
+
+#include <algorithm>
+#include <cstring>
+#include <type_traits>
 
 #include "dense.hpp"
 
 namespace remora {
 namespace cuda {
+
+namespace detail {
+// Lines [a, b) of an m x n expression in the orientation of its storage: rows of a
+// row-major matrix, columns of a column-major one.
+template <class E>
+auto lines(E&& e, std::size_t a, std::size_t b, std::size_t m, std::size_t n, row_major)
+    -> decltype(subrange(std::forward<E>(e), a, b, 0, n)) {
+    return subrange(std::forward<E>(e), a, b, 0, n);
+}
+template <class E>
+auto lines(E&& e, std::size_t a, std::size_t b, std::size_t m, std::size_t n, column_major)
+    -> decltype(subrange(std::forward<E>(e), 0, m, a, b)) {
+    return subrange(std::forward<E>(e), 0, m, a, b);
+}
+// A host matrix over `count` consecutive lines of a staging chunk.
+template <class T, class O>
+remora::dense_matrix_adaptor<T, O> chunk_view(T* p, std::size_t count, std::size_t m, std::size_t n) {
+    const std::size_t minor = O::index_m(m, n);
+    return std::is_same<O, row_major>::value ? remora::dense_matrix_adaptor<T, O>(p, count, n, minor)
+                                             : remora::dense_matrix_adaptor<T, O>(p, m, count, minor);
+}
+// True when M has dense storage in orientation O (its lines can be copied as memory).
+template <class M, class O>
+struct dense_lines
+    : std::integral_constant<bool, std::is_base_of<dense_tag, typename M::storage_type::storage_tag>::value &&
+                                       std::is_same<typename M::orientation, O>::value> {};
+
+// Lines [a, b) of the host expression e into the staging lines at buf.
+template <class O, class E, class T>
+void pack(E const& e, T* buf, std::size_t a, std::size_t b, std::size_t m, std::size_t n, std::true_type) {
+    auto st = e.raw_storage();
+    const std::size_t minor = O::index_m(m, n);
+    for (std::size_t l = a; l != b; ++l)
+        std::memcpy(buf + (l - a) * minor, st.values + l * st.leading_dimension, minor * sizeof(T));
+}
+template <class O, class E, class T>
+void pack(E const& e, T* buf, std::size_t a, std::size_t b, std::size_t m, std::size_t n, std::false_type) {
+    auto view = chunk_view<T, O>(buf, b - a, m, n);
+    noalias(view) = lines(e, a, b, m, n, O());
+}
+// The staging lines at buf into lines [a, b) of the host target x.
+template <class O, class X, class T>
+void unpack(X& x, T const* buf, std::size_t a, std::size_t b, std::size_t m, std::size_t n, std::true_type) {
+    auto st = x.raw_storage();
+    const std::size_t minor = O::index_m(m, n);
+    for (std::size_t l = a; l != b; ++l)
+        std::memcpy(st.values + l * st.leading_dimension, buf + (l - a) * minor, minor * sizeof(T));
+}
+template <class O, class X, class T>
+void unpack(X& x, T const* buf, std::size_t a, std::size_t b, std::size_t m, std::size_t n, std::false_type) {
+    noalias(lines(x, a, b, m, n, O())) = chunk_view<T const, O>(buf, b - a, m, n);
+}
+}  // namespace detail
 
 template <class E>
 class matrix_transport_to_host : public matrix_expression<matrix_transport_to_host<E>, cpu_tag> {
@@ -38,14 +103,46 @@ public:
     template <class MatX>
     void assign_to(matrix_expression<MatX, cpu_tag>& X) const {
         typedef typename MatX::orientation::orientation XO;
-        // A device copy with X's orientation, then one pitched device-to-host copy.
+        const std::size_t m = size1(), n = size2();
+        if (m == 0 || n == 0) return;
+        // A dense device copy in X's orientation, then chunks of its lines through the
+        // page-locked staging: the DMA of chunk k + 1 runs while chunk k is unpacked.
         matrix<value_type, XO, cuda_tag> staged(m_expression);
         device& dev = staged.queue();
-        auto xs = X().raw_storage();
-        const std::size_t major = XO::index_M(size1(), size2()), minor = XO::index_m(size1(), size2());
-        check(rc_memcpy2d(xs.values, xs.leading_dimension * sizeof(value_type), staged.raw_storage().values,
-                          minor * sizeof(value_type), minor * sizeof(value_type), major, RC_COPY_D2H, dev.stream()),
-              "rc_memcpy2d");
+        const std::size_t major = XO::index_M(m, n), minor = XO::index_m(m, n);
+        const std::size_t line = minor * sizeof(value_type);
+        const value_type* src = staged.raw_storage().values;
+        if (line > host_staging::chunk_bytes) {  // a single line larger than a chunk
+            remora::matrix<value_type, XO> host(m, n);
+            check(rc_memcpy2d(host.raw_storage().values, line, src, line, line, major, RC_COPY_D2H, dev.stream()),
+                  "rc_memcpy2d");
+            dev.synchronize();
+            noalias(X) = host;
+            return;
+        }
+        host_staging& st = host_staging::of(dev);
+        const std::size_t per = host_staging::chunk_bytes / line;
+        const std::size_t chunks = (major + per - 1) / per;
+        auto issue = [&](std::size_t k) {
+            const int c = (int)(k & 1);
+            const std::size_t l0 = k * per, nl = std::min(per, major - l0);
+            st.wait(c);
+            check(rc_memcpy2d(st.chunk(c), line, src + l0 * minor, line, line, nl, RC_COPY_D2H, dev.stream()),
+                  "rc_memcpy2d");
+            st.record(c, dev.stream());
+        };
+        issue(0);
+        if (chunks > 1) issue(1);
+        for (std::size_t k = 0; k < chunks; ++k) {
+            const int c = (int)(k & 1);
+            const std::size_t l0 = k * per, nl = std::min(per, major - l0);
+            st.wait(c);
+            value_type const* buf = static_cast<value_type const*>(st.chunk(c));
+            parallel_lines(nl, [&](std::size_t b, std::size_t e) {
+                detail::unpack<XO>(X(), buf + b * minor, l0 + b, l0 + e, m, n, detail::dense_lines<MatX, XO>());
+            });
+            if (k + 2 < chunks) issue(k + 2);
+        }
         dev.synchronize();
     }
     template <class MatX>
@@ -85,15 +182,38 @@ public:
     template <class MatX>
     void assign_to(matrix_expression<MatX, cuda_tag>& X) const {
         typedef typename MatX::orientation::orientation XO;
-        // Host values in X's orientation, one pitched host-to-device copy into a dense
-        // staging matrix, then a device assignment into X (which may be a strided view).
-        remora::matrix<value_type, XO> host(m_expression);
-        matrix<value_type, XO, cuda_tag> staged(size1(), size2(), *m_queue);
-        const std::size_t major = XO::index_M(size1(), size2()), minor = XO::index_m(size1(), size2());
-        check(rc_memcpy2d(staged.raw_storage().values, minor * sizeof(value_type), host.raw_storage().values,
-                          minor * sizeof(value_type), minor * sizeof(value_type), major, RC_COPY_H2D,
-                          m_queue->stream()),
-              "rc_memcpy2d");
+        const std::size_t m = size1(), n = size2();
+        if (m == 0 || n == 0) return;
+        // Chunks of X-oriented lines of the host expression, evaluated by host threads into
+        // a page-locked chunk while the other chunk's DMA runs, into a dense device staging
+        // matrix; then a device assignment into X (which may be a strided view).
+        matrix<value_type, XO, cuda_tag> staged(m, n, *m_queue);
+        const std::size_t major = XO::index_M(m, n), minor = XO::index_m(m, n);
+        const std::size_t line = minor * sizeof(value_type);
+        value_type* dst = staged.raw_storage().values;
+        if (line > host_staging::chunk_bytes) {  // a single line larger than a chunk
+            remora::matrix<value_type, XO> host(m_expression);
+            check(rc_memcpy2d(dst, line, host.raw_storage().values, line, line, major, RC_COPY_H2D,
+                              m_queue->stream()),
+                  "rc_memcpy2d");
+            m_queue->synchronize();
+        } else {
+            host_staging& st = host_staging::of(*m_queue);
+            const std::size_t per = host_staging::chunk_bytes / line;
+            int c = 0;
+            for (std::size_t l0 = 0; l0 < major; l0 += per, c ^= 1) {
+                const std::size_t nl = std::min(per, major - l0);
+                st.wait(c);
+                value_type* buf = static_cast<value_type*>(st.chunk(c));
+                parallel_lines(nl, [&](std::size_t b, std::size_t e) {
+                    detail::pack<XO>(m_expression, buf + b * minor, l0 + b, l0 + e, m, n,
+                                     detail::dense_lines<typename std::decay<expression_closure_type>::type, XO>());
+                });
+                check(rc_memcpy2d(dst + l0 * minor, line, buf, line, line, nl, RC_COPY_H2D, m_queue->stream()),
+                      "rc_memcpy2d");
+                st.record(c, m_queue->stream());
+            }
+        }
         assign(X, staged);
         m_queue->synchronize();
     }

@@ -9,10 +9,17 @@
 
 #include <remora_cuda.h>
 
+#include <algorithm>
+#include <condition_variable>
+#include <cstdint>
+#include <cstddef>
+#include <functional>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <system_error>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -61,6 +68,150 @@ public:
 private:
     int m_id;
 };
+
+/// Two page-locked host chunks of `chunk_bytes` each, with an event per chunk, for the
+/// transport between host expressions and device storage: the host side of chunk i is
+/// filled (or drained) while the DMA of the other chunk runs on the device's stream. One
+/// set per (device, host thread), allocated on first use, like the stream.
+class host_staging {
+public:
+    static constexpr std::size_t chunk_bytes = std::size_t(32) << 20;
+
+    static host_staging& of(device const& dev) {
+        thread_local std::map<int, std::unique_ptr<host_staging>> sets;
+        auto& s = sets[dev.id()];
+        if (!s) s.reset(new host_staging(dev));
+        return *s;
+    }
+    host_staging(host_staging const&) = delete;
+    host_staging& operator=(host_staging const&) = delete;
+    ~host_staging() {
+        for (int c = 0; c < 2; ++c) {
+            if (m_event[c]) {
+                rc_event_synchronize(m_event[c]);
+                rc_event_destroy(m_event[c]);
+            }
+            rc_host_free(m_buf[c]);
+        }
+    }
+    void* chunk(int c) const { return m_buf[c]; }
+    /// Wait until the DMA last recorded for chunk c has finished with it.
+    void wait(int c) {
+        if (m_used[c]) check(rc_event_synchronize(m_event[c]), "rc_event_synchronize");
+        m_used[c] = false;
+    }
+    /// Mark chunk c busy until the work queued so far on `stream` has run.
+    void record(int c, void* stream) {
+        check(rc_event_record(m_event[c], stream), "rc_event_record");
+        m_used[c] = true;
+    }
+
+private:
+    explicit host_staging(device const& dev) {
+        dev.set_device();
+        for (int c = 0; c < 2; ++c) {
+            check(rc_host_alloc(&m_buf[c], chunk_bytes), "rc_host_alloc");
+            check(rc_event_create(&m_event[c]), "rc_event_create");
+        }
+    }
+    void* m_buf[2] = {nullptr, nullptr};
+    void* m_event[2] = {nullptr, nullptr};
+    bool m_used[2] = {false, false};
+};
+
+/// A small pool of host threads (started on first use, half the hardware threads, at most
+/// 7) that, with the calling thread, packs and unpacks the transport's staging chunks:
+/// Remora's CPU assignment is single-threaded, and one thread moves far less than the
+/// link's rate. One job at a time; a job is a set of parts run by whichever thread is free.
+class host_workers {
+public:
+    static host_workers& instance() {
+        static host_workers w;
+        return w;
+    }
+    std::size_t threads() const { return m_threads.size() + 1; }
+    /// f(part) for part in [0, parts), on the pool and the calling thread; returns when all
+    /// parts are done.
+    void run(std::size_t parts, std::function<void(std::size_t)> const& f) {
+        std::lock_guard<std::mutex> one_job(m_run);
+        {
+            std::lock_guard<std::mutex> lock(m_mutex);
+            m_job = &f;
+            m_parts = parts;
+            m_next = 0;
+            m_finished = 0;
+            ++m_generation;
+        }
+        m_wake.notify_all();
+        work();
+        std::unique_lock<std::mutex> lock(m_mutex);
+        m_done.wait(lock, [&] { return m_finished == m_parts; });
+        m_job = nullptr;
+    }
+    ~host_workers() {
+        {
+            std::lock_guard<std::mutex> lock(m_mutex);
+            m_quit = true;
+        }
+        m_wake.notify_all();
+        for (auto& t : m_threads) t.join();
+    }
+
+private:
+    host_workers() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const unsigned n = std::min(7u, hw > 2 ? hw / 2 - 1 : 0u);
+        for (unsigned i = 0; i < n; ++i) m_threads.emplace_back([this] { loop(); });
+    }
+    // Take parts of the current job until none is left.
+    void work() {
+        while (true) {
+            std::size_t p;
+            std::function<void(std::size_t)> const* job;
+            {
+                std::lock_guard<std::mutex> lock(m_mutex);
+                if (!m_job || m_next >= m_parts) return;
+                p = m_next++;
+                job = m_job;
+            }
+            (*job)(p);
+            std::lock_guard<std::mutex> lock(m_mutex);
+            if (++m_finished == m_parts) m_done.notify_all();
+        }
+    }
+    void loop() {
+        std::uint64_t seen = 0;
+        while (true) {
+            {
+                std::unique_lock<std::mutex> lock(m_mutex);
+                m_wake.wait(lock, [&] { return m_quit || m_generation != seen; });
+                if (m_quit) return;
+                seen = m_generation;
+            }
+            work();
+        }
+    }
+    std::vector<std::thread> m_threads;
+    std::mutex m_run, m_mutex;
+    std::condition_variable m_wake, m_done;
+    std::function<void(std::size_t)> const* m_job = nullptr;
+    std::size_t m_parts = 0, m_next = 0, m_finished = 0;
+    std::uint64_t m_generation = 0;
+    bool m_quit = false;
+};
+
+/// Run f(begin, end) over [0, count) in contiguous pieces on the host worker pool.
+template <class F>
+void parallel_lines(std::size_t count, F f) {
+    host_workers& w = host_workers::instance();
+    const std::size_t parts = std::min<std::size_t>(w.threads(), count);
+    if (parts <= 1) {
+        f(std::size_t(0), count);
+        return;
+    }
+    const std::size_t step = (count + parts - 1) / parts;
+    w.run((count + step - 1) / step, [&](std::size_t p) { f(p * step, std::min(count, (p + 1) * step)); });
+}
 
 /// All devices of the machine (hip/device.hpp:85-110).
 class device_manager {

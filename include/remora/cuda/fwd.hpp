@@ -88,6 +88,14 @@ template <bool Upper, bool Unit, class MatA, class VecV>
 void trmv(matrix_expression<MatA, cuda_tag> const& A, vector_expression<VecV, cuda_tag>& v);
 template <bool Upper, bool Unit, class MatA, class MatB>
 void trmm(matrix_expression<MatA, cuda_tag> const& A, matrix_expression<MatB, cuda_tag>& B);
+// LU with partial pivoting A = P L U in place, P the host permutation Remora's
+// pivoting_lu_decomposition keeps (kernels/getrf.hpp:50-59, decompositions.hpp:253-263).
+template <typename MatA, typename VecP>
+void getrf(matrix_expression<MatA, cuda_tag>& A, vector_expression<VecP, cpu_tag>& P);
+// Pivoted Cholesky P^T A P = L L^T in place, returning the rank (kernels/pstrf.hpp:61-70,
+// decompositions.hpp:321-328).
+template <class Triangular, class MatA, class VecP>
+std::size_t pstrf(matrix_expression<MatA, cuda_tag>& A, vector_expression<VecP, cpu_tag>& P);
 }  // namespace kernels
 
 }  // namespace remora

@@ -9,7 +9,10 @@
 #include <cmath>
 #include <cstdint>
 #include <random>
+#include <stdexcept>
 #include <type_traits>
+#include <utility>
+#include <vector>
 
 #include "dense.hpp"
 
@@ -66,6 +69,16 @@ struct blas<double> {
                       std::size_t ldb, void* s) {
         return rc_copy2d_f64(t, m, n, alpha, A, lda, B, ldb, s);
     }
+    static int getrf(int rm, std::size_t n, double* A, std::size_t lda, int* piv, int* info, void* s) {
+        return rc_getrf_f64(rm, n, A, lda, piv, info, s);
+    }
+    static int pstrf(int rm, std::size_t n, double* A, std::size_t lda, int* piv, int* rank, void* s) {
+        return rc_pstrf_f64(rm, n, A, lda, piv, rank, s);
+    }
+    static int gather(std::size_t m, std::size_t n, int const* idx, double const* A, std::ptrdiff_t ars,
+                      std::ptrdiff_t acs, double* B, std::ptrdiff_t brs, std::ptrdiff_t bcs, void* s) {
+        return rc_gather_rows_f64(m, n, idx, A, ars, acs, B, brs, bcs, s);
+    }
 };
 template <>
 struct blas<float> {
@@ -109,6 +122,16 @@ struct blas<float> {
                       std::size_t ldb, void* s) {
         return rc_copy2d_f32(t, m, n, alpha, A, lda, B, ldb, s);
     }
+    static int getrf(int rm, std::size_t n, float* A, std::size_t lda, int* piv, int* info, void* s) {
+        return rc_getrf_f32(rm, n, A, lda, piv, info, s);
+    }
+    static int pstrf(int rm, std::size_t n, float* A, std::size_t lda, int* piv, int* rank, void* s) {
+        return rc_pstrf_f32(rm, n, A, lda, piv, rank, s);
+    }
+    static int gather(std::size_t m, std::size_t n, int const* idx, float const* A, std::ptrdiff_t ars,
+                      std::ptrdiff_t acs, float* B, std::ptrdiff_t brs, std::ptrdiff_t bcs, void* s) {
+        return rc_gather_rows_f32(m, n, idx, A, ars, acs, B, brs, bcs, s);
+    }
 };
 
 /// Per-device status word for potrf (read back to return the pivot, as the reference does).
@@ -124,10 +147,146 @@ inline int* status_word(device& dev) {
     return static_cast<int*>(w.get());
 }
 
+// The order of rows after Remora's sequence of swaps P (include/remora/permutation.hpp:
+// 51-104): forward, row i swapped with row P(i) for i = 0, 1, ...; inverted, the same
+// swaps in reverse. Row i of the result is row order[i] of the input.
+template <class VecP>
+std::vector<int> swap_order(VecP const& P, bool inverted) {
+    const std::size_t n = P.size();
+    std::vector<int> order(n);
+    for (std::size_t i = 0; i != n; ++i) order[i] = (int)i;
+    if (!inverted)
+        for (std::size_t i = 0; i != n; ++i) std::swap(order[i], order[(std::size_t)P(i)]);
+    else
+        for (std::size_t i = n; i != 0; --i) std::swap(order[i - 1], order[(std::size_t)P(i - 1)]);
+    return order;
+}
+
+// Rows of the m x n strided device matrix X (element (i, j) at p + i rs + j cs) reordered
+// to `order` in one gather: X -> a dense copy -> back through the row order.
+template <class T>
+void gather_rows(std::vector<int> const& order, T* p, std::ptrdiff_t rs, std::ptrdiff_t cs, std::size_t m,
+                 std::size_t n, device& dev) {
+    if (m == 0 || n == 0) return;
+    buffer<int> idx(m, dev), ident(m, dev);
+    buffer<T> tmp(m * n, dev);
+    std::vector<int> id(m);
+    for (std::size_t i = 0; i != m; ++i) id[i] = (int)i;
+    check(rc_memcpy2d(idx.get(), m * sizeof(int), order.data(), m * sizeof(int), m * sizeof(int), 1, RC_COPY_H2D,
+                      dev.stream()),
+          "rc_memcpy2d");
+    check(rc_memcpy2d(ident.get(), m * sizeof(int), id.data(), m * sizeof(int), m * sizeof(int), 1, RC_COPY_H2D,
+                      dev.stream()),
+          "rc_memcpy2d");
+    check(blas<T>::gather(m, n, idx.get(), p, rs, cs, tmp.get(), 1, (std::ptrdiff_t)m, dev.stream()),
+          "rc_gather_rows");
+    check(blas<T>::gather(m, n, ident.get(), tmp.get(), 1, (std::ptrdiff_t)m, p, rs, cs, dev.stream()),
+          "rc_gather_rows");
+    dev.synchronize();
+}
+
+// Element strides (rs, cs) of a dense device matrix.
+template <class M>
+std::pair<std::ptrdiff_t, std::ptrdiff_t> strides_of(M const& A) {
+    const std::ptrdiff_t ld = (std::ptrdiff_t)A.raw_storage().leading_dimension;
+    return trans_of<typename M::orientation>() ? std::make_pair(ld, std::ptrdiff_t(1)) : std::make_pair(std::ptrdiff_t(1), ld);
+}
+
 }  // namespace detail
 }  // namespace cuda
 
+// Row and column swaps of cuda_tag matrices and vectors by a host permutation, the
+// device counterparts of include/remora/permutation.hpp:51-104 (found by argument-
+// dependent lookup from Remora's decompositions).
+template <class VecP, class M>
+void swap_rows(vector_expression<VecP, cpu_tag> const& P, matrix_expression<M, cuda_tag>& A) {
+    auto st = cuda::detail::strides_of(A());
+    cuda::detail::gather_rows(cuda::detail::swap_order(P(), false), A().raw_storage().values, st.first, st.second,
+                              A().size1(), A().size2(), A().queue());
+}
+template <class VecP, class M>
+void swap_rows_inverted(vector_expression<VecP, cpu_tag> const& P, matrix_expression<M, cuda_tag>& A) {
+    auto st = cuda::detail::strides_of(A());
+    cuda::detail::gather_rows(cuda::detail::swap_order(P(), true), A().raw_storage().values, st.first, st.second,
+                              A().size1(), A().size2(), A().queue());
+}
+template <class VecP, class M>
+void swap_columns(vector_expression<VecP, cpu_tag> const& P, matrix_expression<M, cuda_tag>& A) {
+    auto st = cuda::detail::strides_of(A());
+    cuda::detail::gather_rows(cuda::detail::swap_order(P(), false), A().raw_storage().values, st.second, st.first,
+                              A().size2(), A().size1(), A().queue());
+}
+template <class VecP, class M>
+void swap_columns_inverted(vector_expression<VecP, cpu_tag> const& P, matrix_expression<M, cuda_tag>& A) {
+    auto st = cuda::detail::strides_of(A());
+    cuda::detail::gather_rows(cuda::detail::swap_order(P(), true), A().raw_storage().values, st.second, st.first,
+                              A().size2(), A().size1(), A().queue());
+}
+template <class VecP, class V>
+void swap_rows(vector_expression<VecP, cpu_tag> const& P, vector_expression<V, cuda_tag>& v) {
+    cuda::detail::gather_rows(cuda::detail::swap_order(P(), false), v().raw_storage().values,
+                              (std::ptrdiff_t)v().raw_storage().stride, std::ptrdiff_t(0), v().size(), 1, v().queue());
+}
+template <class VecP, class V>
+void swap_rows_inverted(vector_expression<VecP, cpu_tag> const& P, vector_expression<V, cuda_tag>& v) {
+    cuda::detail::gather_rows(cuda::detail::swap_order(P(), true), v().raw_storage().values,
+                              (std::ptrdiff_t)v().raw_storage().stride, std::ptrdiff_t(0), v().size(), 1, v().queue());
+}
+
 namespace kernels {
+
+template <typename MatA, typename VecP>
+void getrf(matrix_expression<MatA, cuda_tag>& A, vector_expression<VecP, cpu_tag>& P) {
+    REMORA_SIZE_CHECK(A().size1() == A().size2());
+    REMORA_SIZE_CHECK(P().size() == A().size1());
+    typedef typename MatA::value_type T;
+    const std::size_t n = A().size1();
+    if (n == 0) return;
+    auto sa = A().raw_storage();
+    cuda::device& dev = A().queue();
+    cuda::buffer<int> piv(n, dev), info(1, dev);
+    cuda::check(cuda::detail::blas<T>::getrf(cuda::detail::trans_of<typename MatA::orientation>(), n, sa.values,
+                                             sa.leading_dimension, piv.get(), info.get(), dev.stream()),
+                "rc_getrf");
+    std::vector<int> h(n);
+    int hinfo = 0;
+    cuda::check(rc_memcpy2d(h.data(), n * sizeof(int), piv.get(), n * sizeof(int), n * sizeof(int), 1, RC_COPY_D2H,
+                            dev.stream()),
+                "rc_memcpy2d");
+    cuda::check(rc_memcpy2d(&hinfo, sizeof(int), info.get(), sizeof(int), sizeof(int), 1, RC_COPY_D2H, dev.stream()),
+                "rc_memcpy2d");
+    dev.synchronize();
+    if (hinfo != 0)  // the reference's CPU kernel throws on a zero pivot (kernels/default/getrf.hpp:59)
+        throw std::invalid_argument("[getrf] Matrix is rank deficient or numerically unstable");
+    for (std::size_t i = 0; i != n; ++i) P()(i) = h[i];
+}
+
+template <class Triangular, class MatA, class VecP>
+std::size_t pstrf(matrix_expression<MatA, cuda_tag>& A, vector_expression<VecP, cpu_tag>& P) {
+    REMORA_SIZE_CHECK(A().size1() == A().size2());
+    REMORA_SIZE_CHECK(P().size() == A().size1());
+    typedef typename MatA::value_type T;
+    const std::size_t n = A().size1();
+    if (n == 0) return 0;
+    auto sa = A().raw_storage();
+    cuda::device& dev = A().queue();
+    cuda::buffer<int> piv(n, dev), rank(1, dev);
+    // The upper factor is the lower factor of the transpose (kernels/default/pstrf.hpp:152-160).
+    const int rm = cuda::detail::trans_of<typename MatA::orientation>() ^ (Triangular::is_upper ? 1 : 0);
+    cuda::check(cuda::detail::blas<T>::pstrf(rm, n, sa.values, sa.leading_dimension, piv.get(), rank.get(),
+                                             dev.stream()),
+                "rc_pstrf");
+    std::vector<int> h(n);
+    int hrank = 0;
+    cuda::check(rc_memcpy2d(h.data(), n * sizeof(int), piv.get(), n * sizeof(int), n * sizeof(int), 1, RC_COPY_D2H,
+                            dev.stream()),
+                "rc_memcpy2d");
+    cuda::check(rc_memcpy2d(&hrank, sizeof(int), rank.get(), sizeof(int), sizeof(int), 1, RC_COPY_D2H, dev.stream()),
+                "rc_memcpy2d");
+    dev.synchronize();
+    for (std::size_t i = 0; i != n; ++i) P()(i) = h[i];
+    return (std::size_t)hrank;
+}
 
 template <class MatA, class MatB, class MatC>
 void gemm(matrix_expression<MatA, cuda_tag> const& A, matrix_expression<MatB, cuda_tag> const& B,

@@ -68,8 +68,9 @@ int rc_selftest_wait_timeout(uint64_t limit_ns, void* stream);
  * Device runtime for hosts compiled without the CUDA toolkit (the cuda_tag headers).
  * Replace the HIP runtime plumbing of include/remora/hip/device.hpp:41-180 (device,
  * stream per thread), include/remora/hip/buffer.hpp:41-102 (owning allocation) and the
- * transport of include/remora/hip/copy.hpp:131-410 (here: pitched asynchronous copies;
- * host memory need not be pinned, in which case the copy is synchronous). */
+ * transport of include/remora/hip/copy.hpp:131-410 (here: pitched asynchronous copies
+ * through page-locked staging chunks, rc_host_alloc; a copy from pageable host memory is
+ * synchronous with respect to the host). */
 enum { RC_COPY_H2D = 1, RC_COPY_D2H = 2, RC_COPY_D2D = 3 };
 int rc_device_count(int* count);
 int rc_set_device(int device);
@@ -79,6 +80,14 @@ int rc_free(void* ptr);
 /* Copy `rows` rows of width_bytes bytes; row r of src starts at src + r * spitch. */
 int rc_memcpy2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width_bytes,
                 size_t rows, int kind, void* stream);
+/* Page-locked host memory (the staging chunks of the transport: DMA at the link's rate,
+ * asynchronous with respect to the host) and events to order reuse of such chunks. */
+int rc_host_alloc(void** ptr, size_t bytes);
+int rc_host_free(void* ptr);
+int rc_event_create(void** event);
+int rc_event_record(void* event, void* stream);
+int rc_event_synchronize(void* event);
+int rc_event_destroy(void* event);
 int rc_stream_create(void** stream);
 int rc_stream_destroy(void* stream);
 int rc_stream_synchronize(void* stream);
@@ -347,6 +356,16 @@ int rc_axpby_f64(size_t n, double alpha, const double* x, size_t incx, double be
                  void* stream);
 int rc_axpby_f32(size_t n, float alpha, const float* x, size_t incx, float beta, float* y, size_t incy, void* stream);
 int rc_fill_f32(size_t m, size_t n, float value, float* A, size_t lda, void* stream);
+/* Row gather B(i, j) = A(idx[i], j) for the m x n matrices A and B given by element strides
+ * (element (i, j) at p + i * rs + j * cs; a vector is m x 1, columns are rows of the
+ * transposed strides); idx (device, m ints) must index rows of A, other rows of B are not
+ * written; B must not be A. The device-side row and column swaps of Remora's permutations
+ * (include/remora/permutation.hpp:51-131: swap_rows, swap_rows_inverted,
+ * swap_columns_inverted) for the cuda_tag, applied as one gather. */
+int rc_gather_rows_f64(size_t m, size_t n, const int* idx, const double* A, ptrdiff_t a_rs,
+                       ptrdiff_t a_cs, double* B, ptrdiff_t b_rs, ptrdiff_t b_cs, void* stream);
+int rc_gather_rows_f32(size_t m, size_t n, const int* idx, const float* A, ptrdiff_t a_rs,
+                       ptrdiff_t a_cs, float* B, ptrdiff_t b_rs, ptrdiff_t b_cs, void* stream);
 
 #ifdef __cplusplus
 }

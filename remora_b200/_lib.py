@@ -45,6 +45,12 @@ SIGNATURES: dict[str, list] = {
     "rc_malloc": [_P, _Z],
     "rc_free": [_P],
     "rc_memcpy2d": [_P, _Z, _P, _Z, _Z, _Z, _I, _P],
+    "rc_host_alloc": [_P, _Z],
+    "rc_host_free": [_P],
+    "rc_event_create": [_P],
+    "rc_event_record": [_P, _P],
+    "rc_event_synchronize": [_P],
+    "rc_event_destroy": [_P],
     "rc_stream_create": [_P],
     "rc_stream_destroy": [_P],
     "rc_stream_synchronize": [_P],
@@ -97,6 +103,10 @@ SIGNATURES: dict[str, list] = {
     "rc_copy2d_f64": [_I, _Z, _Z, c_double, _P, _Z, _P, _Z, _P],
     "rc_copy2d_f32": [_I, _Z, _Z, c_float, _P, _Z, _P, _Z, _P],
     "rc_fill_f64": [_Z, _Z, c_double, _P, _Z, _P],
+    "rc_gather_rows_f64": [_Z, _Z, _P, _P, ctypes.c_ssize_t, ctypes.c_ssize_t, _P, ctypes.c_ssize_t,
+                           ctypes.c_ssize_t, _P],
+    "rc_gather_rows_f32": [_Z, _Z, _P, _P, ctypes.c_ssize_t, ctypes.c_ssize_t, _P, ctypes.c_ssize_t,
+                           ctypes.c_ssize_t, _P],
     "rc_fill_f32": [_Z, _Z, c_float, _P, _Z, _P],
 }
 _RESTYPES = {"rc_error_string": ctypes.c_char_p, "rc_launch_count": ctypes.c_ulonglong,

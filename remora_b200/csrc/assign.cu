@@ -40,6 +40,23 @@ __global__ void __launch_bounds__(256) fill_kernel(int64_t m, int64_t n, T value
         }
 }
 
+// B(i, j) = A(idx[i], j): a row gather with arbitrary element strides on both sides (the
+// unit-stride index of B walks threadIdx.x). Rows whose index is outside [0, m) are not
+// written.
+template <class T>
+__global__ void __launch_bounds__(256) gather_rows_kernel(int64_t m, int64_t n, const int* __restrict__ idx,
+                                                          View<const T> A, View<T> B) {
+    const bool col = B.rs == 1;
+    const int64_t inner = col ? m : n, outer = col ? n : m;
+    for (int64_t o = blockIdx.y; o < outer; o += gridDim.y)
+        for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < inner;
+             x += (int64_t)gridDim.x * blockDim.x) {
+            const int64_t i = col ? x : o, j = col ? o : x;
+            const int64_t r = idx[i];
+            if (r >= 0 && r < m) B(i, j) = A(r, j);
+        }
+}
+
 }  // namespace
 
 template <class S, class D>
@@ -85,6 +102,20 @@ int copy_abi(int trans, size_t m, size_t n, T alpha, const T* A, size_t lda, T* 
                             static_cast<cudaStream_t>(stream));
 }
 template <class T>
+int gather_abi(size_t m, size_t n, const int* idx, const T* A, ptrdiff_t ars, ptrdiff_t acs, T* B, ptrdiff_t brs,
+               ptrdiff_t bcs, void* stream) {
+    if (m == 0 || n == 0) return RC_SUCCESS;
+    if (!idx || !A || !B || A == B) return RC_ERR_INVALID_ARGUMENT;
+    const rc::View<T> b{B, (int64_t)brs, (int64_t)bcs};
+    const bool col = brs == 1;
+    const int64_t inner = col ? (int64_t)m : (int64_t)n, outer = col ? (int64_t)n : (int64_t)m;
+    dim3 grid(rc::ceil_div(inner, 256) < 1024u ? rc::ceil_div(inner, 256) : 1024u,
+              outer < 65535 ? (unsigned)outer : 65535u);
+    rc::gather_rows_kernel<T><<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        (int64_t)m, (int64_t)n, idx, rc::View<const T>{A, (int64_t)ars, (int64_t)acs}, b);
+    return rc::check_launch();
+}
+template <class T>
 int fill_abi(size_t m, size_t n, T value, T* A, size_t lda, void* stream) {
     if (m == 0 || n == 0) return RC_SUCCESS;
     if (!A || lda < m) return RC_ERR_INVALID_ARGUMENT;
@@ -100,6 +131,14 @@ int rc_copy2d_f64(int trans, size_t m, size_t n, double alpha, const double* A, 
 int rc_copy2d_f32(int trans, size_t m, size_t n, float alpha, const float* A, size_t lda, float* B, size_t ldb,
                   void* stream) {
     return copy_abi<float>(trans, m, n, alpha, A, lda, B, ldb, stream);
+}
+int rc_gather_rows_f64(size_t m, size_t n, const int* idx, const double* A, ptrdiff_t a_rs, ptrdiff_t a_cs, double* B,
+                       ptrdiff_t b_rs, ptrdiff_t b_cs, void* stream) {
+    return gather_abi<double>(m, n, idx, A, a_rs, a_cs, B, b_rs, b_cs, stream);
+}
+int rc_gather_rows_f32(size_t m, size_t n, const int* idx, const float* A, ptrdiff_t a_rs, ptrdiff_t a_cs, float* B,
+                       ptrdiff_t b_rs, ptrdiff_t b_cs, void* stream) {
+    return gather_abi<float>(m, n, idx, A, a_rs, a_cs, B, b_rs, b_cs, stream);
 }
 int rc_fill_f64(size_t m, size_t n, double value, double* A, size_t lda, void* stream) {
     return fill_abi<double>(m, n, value, A, lda, stream);

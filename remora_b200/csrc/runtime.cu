@@ -1,8 +1,9 @@
 // Device runtime entry points for host code that is compiled without the CUDA toolkit
-// (the header-only cuda_tag containers): device selection, allocation, 2-D copies and
-// streams. They replace the HIP runtime calls of include/remora/hip/device.hpp:41-180
-// and include/remora/hip/buffer.hpp:41-102, and the mapped-memory transport of
-// include/remora/hip/copy.hpp:131-410 (here: pitched cudaMemcpy2DAsync).
+// (the header-only cuda_tag containers): device selection, allocation, 2-D copies,
+// page-locked host staging, events and streams. They replace the HIP runtime calls of
+// include/remora/hip/device.hpp:41-180 and include/remora/hip/buffer.hpp:41-102, and the
+// mapped-memory transport of include/remora/hip/copy.hpp:131-410 (here: pitched
+// cudaMemcpy2DAsync through double-buffered page-locked chunks).
 #include "common.cuh"
 
 namespace {
@@ -47,6 +48,31 @@ int rc_memcpy2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t
     return status_of(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width_bytes, rows, k,
                                        static_cast<cudaStream_t>(stream)));
 }
+
+int rc_host_alloc(void** ptr, size_t bytes) {
+    if (!ptr) return RC_ERR_INVALID_ARGUMENT;
+    *ptr = nullptr;
+    if (bytes == 0) return RC_SUCCESS;
+    return status_of(cudaHostAlloc(ptr, bytes, cudaHostAllocPortable));
+}
+int rc_host_free(void* ptr) { return ptr ? status_of(cudaFreeHost(ptr)) : RC_SUCCESS; }
+
+int rc_event_create(void** event) {
+    if (!event) return RC_ERR_INVALID_ARGUMENT;
+    cudaEvent_t e = nullptr;
+    const int r = status_of(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    *event = e;
+    return r;
+}
+int rc_event_record(void* event, void* stream) {
+    if (!event) return RC_ERR_INVALID_ARGUMENT;
+    return status_of(cudaEventRecord(static_cast<cudaEvent_t>(event), static_cast<cudaStream_t>(stream)));
+}
+int rc_event_synchronize(void* event) {
+    if (!event) return RC_ERR_INVALID_ARGUMENT;
+    return status_of(cudaEventSynchronize(static_cast<cudaEvent_t>(event)));
+}
+int rc_event_destroy(void* event) { return event ? status_of(cudaEventDestroy(static_cast<cudaEvent_t>(event))) : RC_SUCCESS; }
 
 int rc_stream_create(void** stream) {
     if (!stream) return RC_ERR_INVALID_ARGUMENT;

@@ -8,8 +8,10 @@
 #include <remora/cuda.hpp>
 #include <remora/remora.hpp>
 
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <random>
 
 using namespace remora;
@@ -51,6 +53,117 @@ matrix<double> createSymm(std::size_t n) {
     }
     matrix<double> A = prod(R, trans(R));
     return A;
+}
+
+// Test/getrf.cpp:16-30: a matrix whose partial pivoting always picks the next row.
+matrix<double> createLU(std::size_t n) {
+    matrix<double> L(n, n, 0.0), U(n, n, 0.0);
+    for (std::size_t i = 0; i != n; ++i) {
+        for (std::size_t j = 0; j < i; ++j) L(i, j) = 3 - 3.0 / n * std::abs((int)i - (int)j);
+        U(i, i) = 0.5 / n * i + 1;
+        L(i, i) = 1;
+    }
+    matrix<double> A = prod(L, U);
+    return A;
+}
+
+// Test/symm_solve.cpp:17-36: symmetric positive semidefinite of the given rank.
+matrix<double> createSymmRank(std::size_t n, std::size_t rank) {
+    matrix<double> R(n, n, 0.0);
+    for (std::size_t i = 0; i != n; ++i) {
+        for (std::size_t j = 0; j < std::min(i, rank); ++j) R(i, j) = 0.2 / std::abs((int)i - (int)j);
+        if (i < rank) R(i, i) = 0.5 / n * i + 1;
+    }
+    matrix<double> A = prod(R, trans(R));
+    if (rank != n)
+        for (std::size_t i = 0; i != rank / 2; ++i) {
+            A.swap_rows(2 * i, n - i - 1);
+            A.swap_columns(2 * i, n - i - 1);
+        }
+    return A;
+}
+
+// kernels::getrf, pivoting_lu_decomposition and symm_pos_semi_definite_solver on the
+// device (decompositions.hpp:253-263, :321-328) against the same classes on the CPU.
+template <class O>
+void pivoting_tests(char const* tag) {
+    char name[128];
+    {
+        const std::size_t n = 123;  // Test/getrf.cpp:38
+        matrix<double, O> A = createLU(n);
+        permutation_matrix P(n), Pd(n);
+        matrix<double, O> dec = A;
+        kernels::getrf(dec, P);
+        matrix<double, O, cuda_tag> decd = copy_to_device(A, cuda_tag());
+        kernels::getrf(decd, Pd);
+        matrix<double> got = copy_to_cpu(decd);
+        std::size_t same = 0;
+        for (std::size_t i = 0; i != n; ++i) same += P(i) == Pd(i);
+        std::snprintf(name, sizeof(name), "kernels::getrf n=123 %s: pivots as the CPU's", tag);
+        report(name, double(n - same), 0.0);
+        std::snprintf(name, sizeof(name), "kernels::getrf n=123 %s: factors", tag);
+        report(name, rel_diff(got, dec), 1e-13);
+        matrix<double> up(n, n, 0.0);
+        for (std::size_t r = 0; r != n; ++r)
+            for (std::size_t c = r; c != n; ++c) up(r, c) = got(r, c);
+        matrix<double> testA = triangular_prod<unit_lower>(got, up);
+        swap_rows_inverted(Pd, testA);
+        std::snprintf(name, sizeof(name), "kernels::getrf n=123 %s: max|A - P L U| (Test/getrf.cpp)", tag);
+        report(name, max(abs(A - testA)), 1e-12);
+    }
+    {
+        const std::size_t n = 300, k = 7;
+        std::mt19937 gen(31);
+        std::uniform_real_distribution<double> u(0, 1);
+        matrix<double, O> A(n, n), B(n, k), Br(k, n);
+        for (std::size_t i = 0; i != n; ++i)
+            for (std::size_t j = 0; j != n; ++j) A(i, j) = u(gen) + (i == j ? 0.1 : 0.0);
+        for (std::size_t i = 0; i != n; ++i)
+            for (std::size_t j = 0; j != k; ++j) B(i, j) = Br(j, i) = u(gen) - 0.5;
+        pivoting_lu_decomposition<matrix<double, O>> lu(A);
+        matrix<double, O, cuda_tag> Ad = copy_to_device(A, cuda_tag());
+        pivoting_lu_decomposition<matrix<double, O, cuda_tag>> lud(Ad);
+        matrix<double, O> X = B, Xr = Br;
+        lu.solve(X, left());
+        lu.solve(Xr, right());
+        matrix<double, O, cuda_tag> Xd = copy_to_device(B, cuda_tag()), Xrd = copy_to_device(Br, cuda_tag());
+        lud.solve(Xd, left());
+        lud.solve(Xrd, right());
+        std::snprintf(name, sizeof(name), "pivoting_lu_decomposition n=300 %s: A X = B", tag);
+        report(name, rel_diff(matrix<double>(copy_to_cpu(Xd)), X), 1e-12);
+        std::snprintf(name, sizeof(name), "pivoting_lu_decomposition n=300 %s: X A = B", tag);
+        report(name, rel_diff(matrix<double>(copy_to_cpu(Xrd)), Xr), 1e-12);
+        vector<double> b(n), bd_h(n);
+        for (std::size_t i = 0; i != n; ++i) b(i) = B(i, 0);
+        vector<double, cuda_tag> bd = copy_to_device(b, cuda_tag());
+        lu.solve(b, left());
+        lud.solve(bd, left());
+        bd_h = copy_to_cpu(bd);
+        std::snprintf(name, sizeof(name), "pivoting_lu_decomposition n=300 %s: vector solve", tag);
+        report(name, rel_diff(to_matrix(bd_h, 1, n), to_matrix(b, 1, n)), 1e-12);
+    }
+    for (std::size_t rank : {std::size_t(128), std::size_t(50)}) {  // Test/symm_solve.cpp:191, :289
+        const std::size_t n = 128, k = 151;
+        matrix<double> A = createSymmRank(n, rank);
+        matrix<double, O> B(n, k);
+        for (std::size_t i = 0; i != n; ++i)
+            for (std::size_t j = 0; j < k; ++j) B(i, j) = 0.1 * j + (1.0 / n) * i;
+        symm_pos_semi_definite_solver<matrix<double, O>> cpu(A);
+        matrix<double, O, cuda_tag> Ad = copy_to_device(matrix<double, O>(A), cuda_tag());
+        symm_pos_semi_definite_solver<matrix<double, O, cuda_tag>> dev(Ad);
+        std::snprintf(name, sizeof(name), "symm_pos_semi_definite_solver n=128 rank %zu %s: rank", rank, tag);
+        report(name, std::abs(double(dev.rank()) - double(cpu.rank())), 0.0);
+        matrix<double, O> X = B;
+        cpu.solve(X, left());
+        matrix<double, O, cuda_tag> Xd = copy_to_device(B, cuda_tag());
+        dev.solve(Xd, left());
+        matrix<double> Xh = copy_to_cpu(Xd);
+        std::snprintf(name, sizeof(name), "symm_pos_semi_definite_solver n=128 rank %zu %s: X vs CPU", rank, tag);
+        report(name, rel_diff(Xh, X), 1e-10);
+        matrix<double> diff = prod(A, Xh) - B;
+        std::snprintf(name, sizeof(name), "symm_pos_semi_definite_solver rank %zu %s: max|A(AX - B)|", rank, tag);
+        report(name, max(abs(prod(A, diff))), 1e-12);
+    }
 }
 
 template <class OA, class OB, class OC>
@@ -334,6 +447,98 @@ int main() {
         ref *= 0.5;
         report("GP NLL adjoint dF/dK vs Remora CPU 1/2(inv(K) - a a^T)", rel_diff(matrix<double>(copy_to_cpu(Kbar)), ref),
                1e-9);
+    }
+    pivoting_tests<row_major>("row-major");
+    pivoting_tests<column_major>("column-major");
+    {
+        // Transport through the page-locked chunks: several chunks per matrix, both
+        // orientations on both sides, strided (subrange) targets and an expression source;
+        // every element must arrive bit for bit.
+        const std::size_t m = 3001, n = 1537;  // 36.9 MB of FP64: five 8 MiB chunks
+        std::mt19937 gen(77);
+        std::uniform_real_distribution<double> u(-1, 1);
+        matrix<double> A(m, n), B(m, n);
+        for (std::size_t i = 0; i != m; ++i)
+            for (std::size_t j = 0; j != n; ++j) {
+                A(i, j) = u(gen);
+                B(i, j) = u(gen);
+            }
+        matrix<double, column_major, cuda_tag> Ac = copy_to_device(A, cuda_tag());
+        matrix<double, row_major, cuda_tag> Ar = copy_to_device(A, cuda_tag());
+        matrix<double> back_c = copy_to_cpu(Ac), back_r = copy_to_cpu(Ar);
+        matrix<double, column_major> back_cc = copy_to_cpu(Ar);
+        report("transport 3001x1537 FP64 to column-major and back", rel_diff(back_c, A), 0.0);
+        report("transport 3001x1537 FP64 to row-major and back", rel_diff(back_r, A), 0.0);
+        report("transport row-major device to column-major host", rel_diff(back_cc, A), 0.0);
+        matrix<double, row_major, cuda_tag> E = copy_to_device(2.0 * A - B, cuda_tag());
+        matrix<double> Eh = 2.0 * A - B;
+        report("transport of a host expression (2 A - B)", rel_diff(matrix<double>(copy_to_cpu(E)), Eh), 0.0);
+        matrix<double, column_major, cuda_tag> big(m + 40, n + 30, 0.0);
+        noalias(subrange(big, 17, 17 + m, 5, 5 + n)) = copy_to_device(A, cuda_tag());
+        matrix<double> bigh = copy_to_cpu(big);
+        report("transport into a strided device view", rel_diff(matrix<double>(subrange(bigh, 17, 17 + m, 5, 5 + n)), A),
+               0.0);
+        double outside = 0;
+        for (std::size_t i = 0; i != m + 40; ++i)
+            for (std::size_t j = 0; j != n + 30; ++j)
+                if (i < 17 || i >= 17 + m || j < 5 || j >= 5 + n) outside += std::abs(bigh(i, j));
+        report("transport leaves the rest of the device matrix alone", outside, 0.0);
+        matrix<double> hv(m + 3, n + 9, -1.0);
+        noalias(subrange(hv, 2, 2 + m, 4, 4 + n)) = copy_to_cpu(Ac);
+        report("transport into a strided host view", rel_diff(matrix<double>(subrange(hv, 2, 2 + m, 4, 4 + n)), A), 0.0);
+        matrix<float, row_major, cuda_tag> Af = copy_to_device(matrix<float>(A), cuda_tag());
+        report("transport FP32 round trip", rel_diff(matrix<float>(copy_to_cpu(Af)), matrix<float>(A)), 0.0);
+    }
+    {
+        // Transport rates (reported, not checked): a 8192 x 8192 FP64 matrix (512 MiB) to the
+        // device and back through the cuda_tag transports, next to one plain DMA of the same
+        // bytes from page-locked host memory (the link's rate).
+        const std::size_t n = 8192, bytes = n * n * sizeof(double);
+        matrix<double> H(n, n);
+        for (std::size_t i = 0; i != n; ++i)
+            for (std::size_t j = 0; j != n; ++j) H(i, j) = double(i) - 0.5 * double(j);
+        matrix<double, row_major, cuda_tag> D(n, n);
+        cuda::device& dev = device_traits<cuda_tag>::default_queue();
+        auto seconds = [](std::chrono::steady_clock::time_point t0) {
+            return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        };
+        noalias(D) = copy_to_device(H, cuda_tag());  // first use: staging chunks allocated
+        auto t0 = std::chrono::steady_clock::now();
+        noalias(D) = copy_to_device(H, cuda_tag());
+        const double h2d = seconds(t0);
+        matrix<double> H2(n, n);
+        noalias(H2) = copy_to_cpu(D);
+        t0 = std::chrono::steady_clock::now();
+        noalias(H2) = copy_to_cpu(D);
+        const double d2h = seconds(t0);
+        report("transport 8192x8192 FP64 round trip exact", rel_diff(H2, H), 0.0);
+        void* pinned = nullptr;
+        cuda::check(rc_host_alloc(&pinned, bytes), "rc_host_alloc");
+        std::memcpy(pinned, H.raw_storage().values, bytes);
+        cuda::check(rc_memcpy2d(D.raw_storage().values, bytes, pinned, bytes, bytes, 1, RC_COPY_H2D, dev.stream()),
+                    "rc_memcpy2d");
+        dev.synchronize();
+        t0 = std::chrono::steady_clock::now();
+        cuda::check(rc_memcpy2d(D.raw_storage().values, bytes, pinned, bytes, bytes, 1, RC_COPY_H2D, dev.stream()),
+                    "rc_memcpy2d");
+        dev.synchronize();
+        const double link_h2d = seconds(t0);
+        t0 = std::chrono::steady_clock::now();
+        cuda::check(rc_memcpy2d(pinned, bytes, D.raw_storage().values, bytes, bytes, 1, RC_COPY_D2H, dev.stream()),
+                    "rc_memcpy2d");
+        dev.synchronize();
+        const double link_d2h = seconds(t0);
+        rc_host_free(pinned);
+        t0 = std::chrono::steady_clock::now();
+        cuda::check(rc_memcpy2d(D.raw_storage().values, bytes, H.raw_storage().values, bytes, bytes, 1, RC_COPY_H2D,
+                                dev.stream()),
+                    "rc_memcpy2d");
+        dev.synchronize();
+        const double pageable_h2d = seconds(t0);
+        std::printf("transport rate 512 MiB FP64: copy_to_device %.1f GB/s, copy_to_cpu %.1f GB/s; one DMA from "
+                    "page-locked memory H2D %.1f GB/s, D2H %.1f GB/s; one DMA from pageable memory H2D %.1f GB/s\n",
+                    bytes / h2d / 1e9, bytes / d2h / 1e9, bytes / link_h2d / 1e9, bytes / link_d2h / 1e9,
+                    bytes / pageable_h2d / 1e9);
     }
     std::printf("%s (%d failures)\n", failures ? "FAILED" : "PASSED", failures);
     return failures ? 1 : 0;
