@@ -310,6 +310,14 @@ int rc_spd_solve_mixed(int precision, size_t n, size_t nrhs, const double* A, si
  * kernels::syrk<false> of include/remora/kernels/syrk.hpp:55-67, in reduced precision.) */
 int rc_syrk_tc(int precision, size_t n, size_t k, float alpha, const void* P, size_t ldp,
                float beta, float* C, size_t ldc, void* stream);
+/* rc_syrk_tc with options. RC_SYRK_BESIDE: the configuration that leaves room on every SM
+ * for one more tensor-core CTA (a shallower operand ring), for a call that runs beside
+ * other tensor-core work on another stream -- the configuration the mixed factorisation
+ * uses for its trailing updates, whose look-ahead runs beside them. Without it (and in
+ * rc_syrk_tc) the call takes the deeper ring and a whole SM per CTA. */
+enum { RC_SYRK_BESIDE = 1 };
+int rc_syrk_tc_ex(int precision, size_t n, size_t k, float alpha, const void* P, size_t ldp,
+                  float beta, float* C, size_t ldc, int flags, void* stream);
 /* Device workspace the solve caches for these sizes, in bytes. */
 int rc_spd_solve_mixed_workspace(int precision, size_t n, size_t nrhs,
                                  const rc_mixed_options* options, size_t* bytes);

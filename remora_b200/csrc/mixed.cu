@@ -803,7 +803,7 @@ struct Mixed {
                 RC_TRY(ok(cudaStreamWaitEvent(s, ev_packed, 0)));
                 // Two SMs stay free of pair CTAs for the look-ahead's diagonal blocks.
                 RC_TRY(gemm_tc_pair_kmajor(bf16, r2, r2, w, -1.f, op2, ldo, op2, ldo, 1.f, Wm.sub(k1 + w1, k1 + w1),
-                                           kLower, 0, s, info, 2));
+                                           kLower, 0, s, info, 2, true));
                 RC_TRY(ok(cudaEventRecord(ev_t2, s)));
                 t2_pending = true;
             } else {

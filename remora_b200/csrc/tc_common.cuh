@@ -211,9 +211,18 @@ __device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* tm, const v
         "r"(x), "r"(y), "r"(smem_u32(src))
         : "memory");
 }
+__device__ __forceinline__ void tma_reduce_add_3d(const CUtensorMap* tm, const void* src, int x, int y, int z) {
+    asm volatile(
+        "cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tm),
+        "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+        : "memory");
+}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// Wait until at most one of this thread's bulk groups still reads its shared-memory source.
-__device__ __forceinline__ void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+// Wait until at most N of this thread's bulk groups still read their shared-memory sources.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
 // Wait until every bulk group of this thread has completed.
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // Order this thread's shared-memory writes before later bulk copies that read them.

@@ -231,61 +231,108 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 // of the next tile wait on its tempty barrier, which both CTAs' epilogue groups arrive on
 // once their TMEM reads are done.
 //
-// Epilogue. Fast path (beta = 1, C row-major and 16-byte aligned, tile off the diagonal):
-// each epilogue warp moves its 32 rows 16 columns at a time TMEM -> registers (x alpha) ->
-// a 64-byte-swizzled staging box in shared memory -> a TMA reduce-add into C, with two
-// staging boxes per warp in flight; C is never read by the SM. Otherwise the rows are
-// finished element by element (the triangle mask, general beta).
+// Epilogue. Four warps, one per TMEM lane quadrant (warp w may read lanes 32 (w mod 4) ..),
+// each finishing the 256 columns of its 32 rows. Fast path (beta = 1, C row-major and
+// 16-byte aligned with a multiple of 32 columns, tile off the diagonal): TMEM -> registers
+// (x alpha) -> a staging box in shared memory (32 rows x EPI_BLK blocks of 32 columns,
+// 128-byte swizzled) -> one TMA reduce-add of the box into C through a 3-D tensor map
+// (column-in-block, row, column block), EPI_BUFS boxes per warp in flight; C is never read
+// by the SM. The boxes are large because the TMA unit serialises its operations: with 2 KB
+// boxes the reduce-adds of one tile (64 per CTA) took as long as a third of its MMAs.
+// Otherwise the rows are finished element by element (the triangle mask, general beta).
 //
 // One CTA per SM. The shared-memory footprint is at least half an SM's, so no SM holds two
 // pair CTAs and no TPC holds two pairs. (Two pairs on one TPC can allocate TMEM in crossed
 // order -- each pair holding on one SM the columns the other pair waits for on the other
 // SM -- and then both wait forever.) A single-CTA tcgen05 kernel (at most 256 columns, it
 // waits on no other CTA) may run beside a pair CTA; the pair's collective allocation then
-// waits at most until that CTA finishes.
+// waits at most until that CTA finishes. Two configurations:
+//   PairCo    (3 stages, one 32-column box per warp, 113 KB): leaves room beside it for one
+//             single-CTA tcgen05 kernel (~97 KB) -- the factorisation's look-ahead chain
+//             runs there;
+//   PairAlone (5 stages, two 64-column boxes per warp, 225 KB): a deeper ring for a launch
+//             that runs alone (rc_syrk_tc).
 //
 // Failure handling. Every mbarrier wait is bounded and gives up as soon as the device
 // error word or the abort word is raised; the epilogue warps take each decision together
-// (a barrier-reduction over their 128 threads). The two CTAs may still take different
+// (a barrier-reduction over their threads). The two CTAs may still take different
 // decisions, so neither returns early: each reaches the closing cluster barrier, having
 // written its stop flag into both CTAs' `any_stop`; when either stopped, both stay
 // resident for a settle period so that copies still in flight land first.
-constexpr int PAIR_STAGES = 3;
 constexpr int PAIR_A_BYTES = 128 * KB_BYTES, PAIR_B_BYTES = 128 * KB_BYTES;
-constexpr int EPI_COLS = 16;                        // columns of one staged box (64 bytes of FP32)
-constexpr int EPI_BOX_BYTES = 32 * EPI_COLS * 4;    // 32 rows x 16 columns: 2 KB
-constexpr int EPI_BUFS = 2;                         // staged boxes in flight per warp
-constexpr int PAIR_STAGING_BYTES = 4 * EPI_BUFS * EPI_BOX_BYTES;
-constexpr size_t PAIR_SMEM_BASE =
-    1024 + (size_t)PAIR_STAGES * (PAIR_A_BYTES + PAIR_B_BYTES) + PAIR_STAGING_BYTES + 256;
+constexpr int PAIR_THREADS = 192;
+template <int STAGES_, int EPI_BLK_, int EPI_BUFS_>
+struct PairCfg {
+    static constexpr int STAGES = STAGES_;
+    static constexpr int EPI_BLK = EPI_BLK_;                   // 32-column blocks per staged box
+    static constexpr int EPI_COLS = 32 * EPI_BLK;              // columns per box
+    static constexpr int EPI_BOX_BYTES = 32 * EPI_COLS * 4;    // 32 rows
+    static constexpr int EPI_BUFS = EPI_BUFS_;                 // boxes in flight per warp
+    static constexpr int STAGING = 4 * EPI_BUFS * EPI_BOX_BYTES;
+    static constexpr size_t SMEM = 1024 + (size_t)STAGES * (PAIR_A_BYTES + PAIR_B_BYTES) + STAGING + 256;
+};
+// 115,968 bytes: with the 1 KB the hardware reserves per CTA, a 99,584-byte single-CTA
+// kernel still fits beside it in an SM's 233,472.
+using PairCo = PairCfg<3, 1, 1>;
+using PairAlone = PairCfg<5, 2, 2>;
+static_assert(PairCo::SMEM + 1024 + 99584 + 1024 <= 233472, "a look-ahead CTA must fit beside a pair CTA");
 
-// The tile enumeration of one pair launch: mode 0 all tm_count x tn_count tiles (row by
-// row), mode 1 the tiles (tm, tn) with tn <= tm of a square grid, mode 2 those with tn >= tm.
+// The tile enumeration of one pair launch: mode 0 all tm_count x tn_count tiles, mode 1
+// the tiles (tm, tn) with tn <= tm of a square grid, mode 2 those with tn >= tm. Tiles are
+// grouped into blocks of kGroup x kGroup (kGroup tile rows, taken block by block along them,
+// row by row inside a block; triangular blocks on the diagonal), so that the clusters,
+// which take consecutive tiles, share a few A and B row blocks in L2 at any time instead
+// of sweeping the whole panel once per tile row.
+constexpr int64_t kGroup = 8;
 struct PairTiles {
     int mode;
     int64_t tm_count, tn_count, total;
 };
 
-__device__ __forceinline__ void pair_tile(const PairTiles& pt, int64_t t, int64_t& tm, int64_t& tn) {
-    if (pt.mode == 0) {
-        tm = t / pt.tn_count;
-        tn = t % pt.tn_count;
-        return;
-    }
+__device__ __forceinline__ int64_t tri_row(int64_t t) {  // r with r(r+1)/2 <= t < (r+1)(r+2)/2
     int64_t r = (int64_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
     while ((r + 1) * (r + 2) / 2 <= t) ++r;
     while (r * (r + 1) / 2 > t) --r;
-    tm = r;
-    tn = t - r * (r + 1) / 2;
-    if (pt.mode == 2) {
-        const int64_t x = tm;
-        tm = tn;
-        tn = x;
+    return r;
+}
+
+__device__ __forceinline__ void pair_tile(const PairTiles& pt, int64_t t, int64_t& tm, int64_t& tn) {
+    for (int64_t sr = 0;; ++sr) {  // super row sr: tile rows [kGroup sr, kGroup sr + r)
+        const int64_t r0 = kGroup * sr;
+        const int64_t r = pt.tm_count - r0 < kGroup ? pt.tm_count - r0 : kGroup;
+        const int64_t full_blocks = pt.mode == 0 ? pt.tn_count / kGroup : sr;  // r x kGroup blocks
+        const int64_t tail = pt.mode == 0 ? pt.tn_count - full_blocks * kGroup : 0;  // a last narrower block
+        const int64_t diag = pt.mode == 0 ? 0 : r * (r + 1) / 2;
+        const int64_t count = full_blocks * r * kGroup + tail * r + diag;
+        if (t >= count) {
+            t -= count;
+            continue;
+        }
+        if (t < full_blocks * r * kGroup) {
+            const int64_t blk = t / (r * kGroup), in = t % (r * kGroup);
+            tm = r0 + in / kGroup;
+            tn = blk * kGroup + in % kGroup;
+        } else if (pt.mode == 0) {
+            const int64_t in = t - full_blocks * r * kGroup;
+            tm = r0 + in / tail;
+            tn = full_blocks * kGroup + in % tail;
+        } else {
+            const int64_t in = t - full_blocks * r * kGroup;
+            const int64_t a = tri_row(in);
+            tm = r0 + a;
+            tn = r0 + (in - a * (a + 1) / 2);
+        }
+        if (pt.mode == 2) {
+            const int64_t x = tm;
+            tm = tn;
+            tn = x;
+        }
+        return;
     }
 }
 
-template <bool BF16>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
+template <bool BF16, class Cfg>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
     tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                         const __grid_constant__ CUtensorMap tmC, int64_t M, int64_t N, int64_t K, float alpha,
                         float beta, View<float> C, Mask mask, PairTiles pt, int fast, const int* abort, int* err,
@@ -295,9 +342,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;
+    constexpr int PAIR_STAGES = Cfg::STAGES, EPI_COLS = Cfg::EPI_COLS, EPI_BOX_BYTES = Cfg::EPI_BOX_BYTES;
+    constexpr int EPI_BUFS = Cfg::EPI_BUFS;
     uint8_t* sB = sA + PAIR_STAGES * PAIR_A_BYTES;
-    uint8_t* stage_c = sB + PAIR_STAGES * PAIR_B_BYTES;  // 4 warps x EPI_BUFS boxes, 2 KB each
-    uint64_t* full = reinterpret_cast<uint64_t*>(stage_c + PAIR_STAGING_BYTES);
+    uint8_t* stage_c = sB + PAIR_STAGES * PAIR_B_BYTES;  // 4 warps x EPI_BUFS boxes
+    uint64_t* full = reinterpret_cast<uint64_t*>(stage_c + Cfg::STAGING);
     uint64_t* empty = full + PAIR_STAGES;
     uint64_t* tfull = empty + PAIR_STAGES;
     uint64_t* tempty = tfull + 1;
@@ -397,13 +446,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
         }
     } else {
         const int q = warp & 3;  // TMEM lane quadrant this warp may access
+        constexpr int EPI_THREADS = 128;
         uint8_t* my_stage = stage_c + q * EPI_BUFS * EPI_BOX_BYTES;
         const bool vec = C.cs == 1 && (C.rs % 4 == 0) && (reinterpret_cast<uintptr_t>(C.p) % 16 == 0);
         int it = 0, issued = 0;
         for (int64_t t = cluster; t < pt.total; t += nclusters, ++it) {
             const int w = mbar_wait_bounded(tfull, (uint32_t)(it & 1), stop, err, abort, limit_ns);
-            // One decision for the four epilogue warps (their barrier below counts all 128).
-            if (epilogue_any(w != kWaitOk || *stop, 128)) {
+            // One decision for all epilogue warps (their barrier below counts them all).
+            if (epilogue_any(w != kWaitOk || *stop, EPI_THREADS)) {
                 if (w != kWaitOk) raise_stop(stop, err, w, site + kRoleEpilogue * 10);
                 else *stop = 1;
                 break;
@@ -420,23 +470,35 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
                 for (int c0 = 0; c0 < 256; c0 += EPI_COLS) {
                     float v[16];
                     tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
-                    uint8_t* box = my_stage + (issued & (EPI_BUFS - 1)) * EPI_BOX_BYTES;
-                    if (issued >= EPI_BUFS) {  // the box written two steps ago has been read
-                        if (lane == 0) bulk_wait_read_1();
+                    uint8_t* box = my_stage + (issued % EPI_BUFS) * EPI_BOX_BYTES;
+                    if (issued >= EPI_BUFS) {  // the box written EPI_BUFS steps ago has been read
+                        if (lane == 0) bulk_wait_read<EPI_BUFS - 1>();
                         __syncwarp();
                     }
-                    // row `lane` of the box: 64 bytes, 16-byte chunks swizzled by (row / 2) mod 4
+                    // block b of the box: 32 rows x 128 bytes, 16-byte chunks swizzled by row mod 8
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
-                        const int chunk = u ^ ((lane >> 1) & 3);
-                        *reinterpret_cast<float4*>(box + lane * 64 + chunk * 16) =
+                        const int chunk = u ^ (lane & 7);
+                        *reinterpret_cast<float4*>(box + lane * 128 + chunk * 16) =
                             make_float4(alpha * v[4 * u], alpha * v[4 * u + 1], alpha * v[4 * u + 2],
                                         alpha * v[4 * u + 3]);
+                    }
+#pragma unroll
+                    for (int sub = 16; sub < EPI_COLS; sub += 16) {
+                        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(c0 + sub), v);
+                        uint8_t* blk = box + (sub / 32) * 4096;
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int chunk = (((sub % 32) / 4) + u) ^ (lane & 7);
+                            *reinterpret_cast<float4*>(blk + lane * 128 + chunk * 16) =
+                                make_float4(alpha * v[4 * u], alpha * v[4 * u + 1], alpha * v[4 * u + 2],
+                                            alpha * v[4 * u + 3]);
+                        }
                     }
                     fence_proxy_async_smem();
                     __syncwarp();
                     if (lane == 0) {
-                        tma_reduce_add_2d(&tmC, box, (int)(n0 + c0), (int)r0);
+                        tma_reduce_add_3d(&tmC, box, 0, (int)r0, (int)((n0 + c0) / 32));
                         bulk_commit();
                     }
                     ++issued;
@@ -476,7 +538,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
             }
             // This CTA's reads of the accumulator are done: release it to the leader's MMAs.
             tc_fence_before();
-            asm volatile("bar.sync 1, 128;" ::: "memory");
+            asm volatile("bar.sync 1, %0;" ::"r"(EPI_THREADS) : "memory");
             if (warp == 2 && lane == 0) mbar_arrive_cluster(tempty, 0);
         }
         if (lane == 0) bulk_wait_all();  // every reduce-add of this warp has landed
@@ -550,38 +612,37 @@ bool make_tmap(CUtensorMap* tm, const void* base, bool bf16, int64_t rows, int64
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Tensor map of a row-major FP32 C (rows x cols, row stride ld) for the pair epilogue's
-// reduce-adds: 32-row x 16-column boxes, 64-byte swizzle (the staging layout).
-bool make_c_tmap(CUtensorMap* tm, const float* base, int64_t rows, int64_t cols, int64_t ld) {
+// Tensor map of a row-major FP32 C (rows x cols, row stride ld, cols a multiple of 32) for
+// the pair epilogue's reduce-adds, as (column within a 32-column block, row, block): boxes
+// of 32 rows x blk blocks, 128-byte swizzle (the staging layout).
+bool make_c_tmap(CUtensorMap* tm, const float* base, int64_t rows, int64_t cols, int64_t ld, int blk) {
     auto enc = encoder();
-    if (!enc) return false;
-    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
-    cuuint32_t box[2] = {(cuuint32_t)EPI_COLS, 32u};
-    cuuint32_t estr[2] = {1, 1};
-    return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+    if (!enc || cols % 32) return false;
+    cuuint64_t dims[3] = {32u, (cuuint64_t)rows, (cuuint64_t)(cols / 32)};
+    cuuint64_t strides[2] = {(cuuint64_t)ld * 4, 128u};
+    cuuint32_t box[3] = {32u, 32u, (cuuint32_t)blk};
+    cuuint32_t estr[3] = {1, 1, 1};
+    return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Dynamic shared memory of a pair CTA: the ring, the staging boxes and the barriers, and at
-// least half of an SM's shared memory so that no SM ever holds two pair CTAs.
-size_t pair_smem_bytes() {
-    static size_t bytes[64] = {};
+// Dynamic shared memory of a pair CTA: the configuration's ring, staging boxes and barriers,
+// and at least half of an SM's shared memory so that no SM ever holds two pair CTAs.
+size_t pair_smem_bytes(size_t base) {
+    static int per_sm[64] = {}, reserved[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
-    if (!bytes[dev]) {
-        int per_sm = 0, reserved = 0;
-        if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess)
+    if (!per_sm[dev]) {
+        if (cudaDeviceGetAttribute(&per_sm[dev], cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&reserved[dev], cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess)
             return 0;
-        const size_t half = (size_t)per_sm / 2 + 16 - (size_t)reserved;  // two such CTAs do not fit
-        bytes[dev] = PAIR_SMEM_BASE > half ? PAIR_SMEM_BASE : (half + 127) / 128 * 128;
     }
-    return bytes[dev];
+    const size_t half = (size_t)per_sm[dev] / 2 + 16 - (size_t)reserved[dev];  // two such CTAs do not fit
+    return base > half ? base : (half + 127) / 128 * 128;
 }
 
-template <bool BF16>
+template <bool BF16, class Cfg>
 int launch_tc_pair(const CUtensorMap& ta, const CUtensorMap& tb, int64_t m, int64_t n, int64_t k, float alpha,
                    float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s, const int* abort,
                    int reserve_sms) {
@@ -600,15 +661,15 @@ int launch_tc_pair(const CUtensorMap& ta, const CUtensorMap& tb, int64_t m, int6
     CUtensorMap tc;
     std::memset(&tc, 0, sizeof(tc));
     const bool fast = beta == 1.f && C.cs == 1 && C.rs % 4 == 0 && reinterpret_cast<uintptr_t>(C.p) % 16 == 0 &&
-                      make_c_tmap(&tc, C.p, m, n, C.rs);
-    const size_t smem = pair_smem_bytes();
+                      make_c_tmap(&tc, C.p, m, n, C.rs, Cfg::EPI_BLK);
+    const size_t smem = pair_smem_bytes(Cfg::SMEM);
     if (smem == 0 || smem > 232448) return RC_ERR_NOT_SUPPORTED;
-    if (cudaFuncSetAttribute(tc_gemm_pair_kernel<BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(tc_gemm_pair_kernel<BF16, Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
         return RC_ERR_CUDA;
     const int64_t avail = (int64_t)(sm_count() - (reserve_sms > 0 ? reserve_sms : 0)) / 2;
     const int64_t clusters = pt.total < (avail > 0 ? avail : 1) ? pt.total : (avail > 0 ? avail : 1);
-    tc_gemm_pair_kernel<BF16><<<(unsigned)(2 * clusters), TC_THREADS, smem, s>>>(
+    tc_gemm_pair_kernel<BF16, Cfg><<<(unsigned)(2 * clusters), PAIR_THREADS, smem, s>>>(
         ta, tb, tc, m, n, k, alpha, beta, C, mask, pt, fast ? 1 : 0, abort, error_word(), wait_limit_ns());
     return check_launch();
 }
@@ -654,7 +715,7 @@ int gemm_tc_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, cons
 
 int gemm_tc_pair_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, const void* A, int64_t lda,
                         const void* B, int64_t ldb, float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s,
-                        const int* abort, int reserve_sms) {
+                        const int* abort, int reserve_sms, bool beside) {
     if (m <= 0 || n <= 0) return RC_SUCCESS;
     const int es = bf16 ? 2 : 4;
     if (k <= 0 || (reinterpret_cast<uintptr_t>(A) % 16) || (reinterpret_cast<uintptr_t>(B) % 16) || ((lda * es) % 16) ||
@@ -662,8 +723,11 @@ int gemm_tc_pair_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha,
         return RC_ERR_NOT_SUPPORTED;
     CUtensorMap ta, tb;
     if (!make_tmap(&ta, A, bf16, m, k, lda, 128) || !make_tmap(&tb, B, bf16, n, k, ldb, 128)) return RC_ERR_NOT_SUPPORTED;
-    return bf16 ? launch_tc_pair<true>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort, reserve_sms)
-                : launch_tc_pair<false>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort, reserve_sms);
+    if (beside)
+        return bf16 ? launch_tc_pair<true, PairCo>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort, reserve_sms)
+                    : launch_tc_pair<false, PairCo>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort, reserve_sms);
+    return bf16 ? launch_tc_pair<true, PairAlone>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort, reserve_sms)
+                : launch_tc_pair<false, PairAlone>(ta, tb, m, n, k, alpha, beta, C, mask, off, s, abort, reserve_sms);
 }
 
 int gemm_tc_fold_kmajor(int64_t m, int64_t k, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
@@ -764,9 +828,10 @@ int rc_gemm_bf16(int transA, int transB, size_t m, size_t n, size_t k, float alp
                               rc::colmajor(C, (int64_t)ldc), rc::kFull, 0, s);
 }
 
-int rc_syrk_tc(int precision, size_t n, size_t k, float alpha, const void* P, size_t ldp, float beta, float* C,
-               size_t ldc, void* stream) {
+int rc_syrk_tc_ex(int precision, size_t n, size_t k, float alpha, const void* P, size_t ldp, float beta, float* C,
+                  size_t ldc, int flags, void* stream) {
     if (precision != RC_PREC_TF32 && precision != RC_PREC_BF16) return RC_ERR_INVALID_ARGUMENT;
+    if (flags & ~RC_SYRK_BESIDE) return RC_ERR_INVALID_ARGUMENT;
     if (n == 0) return RC_SUCCESS;
     if (!C || ldc < n || (k > 0 && (!P || ldp < k))) return RC_ERR_INVALID_ARGUMENT;
     const bool bf16 = precision == RC_PREC_BF16;
@@ -774,9 +839,15 @@ int rc_syrk_tc(int precision, size_t n, size_t k, float alpha, const void* P, si
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (k > 0 && n >= 256)  // CTA pairs on 256 x 256 tiles
         return rc::gemm_tc_pair_kmajor(bf16, (int64_t)n, (int64_t)n, (int64_t)k, alpha, P, (int64_t)ldp, P,
-                                       (int64_t)ldp, beta, Cv, rc::kLower, 0, s);
+                                       (int64_t)ldp, beta, Cv, rc::kLower, 0, s, nullptr, 0,
+                                       (flags & RC_SYRK_BESIDE) != 0);
     return rc::gemm_tc_kmajor(bf16, (int64_t)n, (int64_t)n, (int64_t)k, alpha, P, (int64_t)ldp, P, (int64_t)ldp, beta,
                               Cv, rc::kLower, 0, s);
+}
+
+int rc_syrk_tc(int precision, size_t n, size_t k, float alpha, const void* P, size_t ldp, float beta, float* C,
+               size_t ldc, void* stream) {
+    return rc_syrk_tc_ex(precision, n, k, alpha, P, ldp, beta, C, ldc, 0, stream);
 }
 
 int rc_selftest_wait_timeout(uint64_t limit_ns, void* stream) {

@@ -17,11 +17,13 @@ int gemm_tc_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, cons
 // SM of the 128 x 256 tiles; with beta = 1 and a row-major 16-byte-aligned C the epilogue
 // adds into C with TMA reduce-adds. Masks: kFull, or kLower / kUpper with off = 0 and
 // m = n (else RC_ERR_NOT_SUPPORTED). reserve_sms SMs are left to kernels that need a whole
-// SM's shared memory (the factorisation's diagonal blocks). abort (device int, may be
-// null): when non-zero the pairs stop (C is then left partly updated).
+// SM's shared memory (the factorisation's diagonal blocks). beside: the configuration that
+// leaves room on every SM for one single-CTA tcgen05 kernel (for a launch that runs beside
+// other tensor-core work); otherwise the deeper-ring configuration. abort (device int, may
+// be null): when non-zero the pairs stop (C is then left partly updated).
 int gemm_tc_pair_kmajor(bool bf16, int64_t m, int64_t n, int64_t k, float alpha, const void* A, int64_t lda,
                         const void* B, int64_t ldb, float beta, View<float> C, Mask mask, int64_t off, cudaStream_t s,
-                        const int* abort = nullptr, int reserve_sms = 0);
+                        const int* abort = nullptr, int reserve_sms = 0, bool beside = false);
 
 // C (m x 64) = alpha * (A B^T folded) + beta * C for a 128-row K-major B = [B_hi; B_lo]:
 // column j of the product is A B_hi(j)^T + A B_lo(j)^T, i.e. A times B_hi + B_lo with

@@ -125,29 +125,33 @@ def test_timeout_is_sticky_and_stops_every_tensor_core_kernel(cuda):
     assert lib.rc_device_status(stream) == 0
 
 
-def _syrk_tc(prec: int, P: torch.Tensor, C: torch.Tensor, alpha: float, beta: float) -> None:
+def _syrk_tc(prec: int, P: torch.Tensor, C: torch.Tensor, alpha: float, beta: float, flags: int = 0) -> None:
     """P is a row-major n x k view whose row stride is a multiple of 16 bytes (the TMA rule)."""
     n, k = P.shape
-    _lib.call("rc_syrk_tc", prec, n, k, alpha, ctypes.c_void_p(P.data_ptr()), P.stride(0), beta,
-              ctypes.c_void_p(C.data_ptr()), n, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    _lib.call("rc_syrk_tc_ex", prec, n, k, alpha, ctypes.c_void_p(P.data_ptr()), P.stride(0), beta,
+              ctypes.c_void_p(C.data_ptr()), n, flags, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
 
 
-@pytest.mark.parametrize("n,k", [(255, 64), (256, 32), (600, 100), (1024, 1024), (1500, 96)])
+@pytest.mark.parametrize("n,k", [(255, 64), (256, 32), (600, 100), (1024, 1024), (1500, 96), (2560, 512)])
 @pytest.mark.parametrize("bf16", [False, True])
-def test_syrk_tc_lower(cuda, n, k, bf16):
+@pytest.mark.parametrize("flags", [0, 1])
+def test_syrk_tc_lower(cuda, n, k, bf16, flags):
     """Lower SYRK C <- alpha P P^T + beta C on the tcgen05 tensor cores (n >= 256 runs on CTA
-    pairs, 256 x 256 tiles); the strict upper triangle of C stays bit-identical."""
+    pairs, 256 x 256 tiles; flags 1 = RC_SYRK_BESIDE, the factorisation's configuration; a
+    multiple of 32 columns takes the reduce-add epilogue when beta = 1); the strict upper
+    triangle of C stays bit-identical."""
     g = torch.Generator(device="cuda").manual_seed(n + k + int(bf16))
     P = torch.rand((n, k), generator=g, device="cuda") * 2 - 1
     C = torch.rand((n, n), generator=g, device="cuda") * 2 - 1
     Pq = P.bfloat16().float() if bf16 else _tf32(P)
-    ref = (-0.75 * (Pq.double() @ Pq.double().t()) + 1.25 * C.double()).tril()
-    Cd = C.clone()
     ld = (k + 15) // 16 * 16  # padded rows
     Pbuf = torch.zeros((n, ld), device="cuda", dtype=torch.bfloat16 if bf16 else torch.float32)
     Pbuf[:, :k] = P.bfloat16() if bf16 else P
-    _syrk_tc(1 if bf16 else 0, Pbuf[:, :k], Cd, -0.75, 1.25)
-    torch.cuda.synchronize()
-    assert _rel(Cd.tril(), ref) <= TC_TOL
-    assert torch.equal(Cd.triu(1), C.triu(1))
+    for beta in (1.25, 1.0):  # beta = 1: the reduce-add epilogue where the shape allows
+        ref = (-0.75 * (Pq.double() @ Pq.double().t()) + beta * C.double()).tril()
+        Cd = C.clone()
+        _syrk_tc(1 if bf16 else 0, Pbuf[:, :k], Cd, -0.75, beta, flags)
+        torch.cuda.synchronize()
+        assert _rel(Cd.tril(), ref) <= TC_TOL
+        assert torch.equal(Cd.triu(1), C.triu(1))
     assert _lib.lib().rc_device_status(None) == 0
