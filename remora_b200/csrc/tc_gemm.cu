@@ -558,17 +558,25 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
     if (threadIdx.x == 0 && *any_stop) settle(kSettleNs);
 }
 
-// Split x into TF32 high part (low 13 mantissa bits cleared) and the FP32 remainder,
-// writing K-major copies: dst row r = [hi(.., k) | hi or lo | ...] per `pattern`.
-// Operand layout in dst (rows x 3K, ld = ldd): segments s = 0, 1, 2 of width K hold
-// part[pattern[s]] (0 = hi, 1 = lo).
+// x rounded to the nearest TF32 value (10 explicit mantissa bits, the low 13 bits zero;
+// ties away from zero): exactly what the tensor cores read from a kind::tf32 operand.
+__device__ __forceinline__ float tf32_rn(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// Split x into hi = tf32_rn(x) and lo = tf32_rn(x - hi) (x - hi is exact in FP32 and below
+// half an ulp of hi, so |x - hi - lo| <= 2^-22 |x|), writing K-major copies: dst row r =
+// [part(p0) | part(p1) | part(p2)], each segment of width K (0 = hi, 1 = lo). Both parts
+// are TF32 values, so the tensor cores drop none of their bits.
 __global__ void split3_kernel(int64_t rows, int64_t K, View<const float> X, float* dst, int64_t ldd, int p0, int p1,
                               int p2) {
     for (int64_t r = blockIdx.y; r < rows; r += gridDim.y)
         for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
             const float x = X(r, k);
-            const float hi = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
-            const float lo = x - hi;
+            const float hi = tf32_rn(x);
+            const float lo = tf32_rn(x - hi);
             float* row = dst + r * ldd;
             row[k] = p0 ? lo : hi;
             row[K + k] = p1 ? lo : hi;
@@ -787,6 +795,9 @@ int gemm_tf32(int64_t m, int64_t n, int64_t k, float alpha, View<const float> A,
         pack_kmajor_kernel<float><<<gb, 256, 0, s>>>(n, k, Bt, b, ld, false);
     }
     RC_TRY(check_launch());
+    // CTA pairs on 256 x 256 tiles where the pair kernel takes the mask; else 128-row tiles.
+    if (m >= 256 && n >= 256 && (mask == kFull || (off == 0 && m == n)))
+        return gemm_tc_pair_kmajor(false, m, n, kk, alpha, a, ld, b, ld, beta, C, mask, off, s, abort, 0, false);
     return gemm_tc_kmajor(false, m, n, kk, alpha, a, ld, b, ld, beta, C, mask, off, s, abort, 0);
 }
 
