@@ -51,6 +51,7 @@ int rc_release_workspaces(void);
  * set here (default 2 s), i.e. at least that long at SM clocks up to 2 GHz. A wait that
  * runs out records RC_ERR_TIMEOUT and where it happened (kernel * 100 + role * 10 + CTA
  * rank in its cluster; kernels 1 = tcgen05 GEMM, 2 = CTA-pair GEMM, 3 = int8 product,
+ * 4 = int8 digit-product trailing update,
  * 9 = self-test; roles 0 = loads, 1 = MMAs, 2 = epilogue) in a per-device error word and
  * its kernel returns, leaving the context usable. The word is sticky: while it is set,
  * every tensor-core kernel returns at once and waits in flight give up, and
@@ -278,10 +279,17 @@ int rc_batched_release_plans(void);
  *    cores on an exact digit split of A (as rc_gemm_f64_sliced, rows and columns scaled
  *    from the diagonal), which adds 8 n^2 bytes to the workspace; every residual that
  *    decides convergence is an FP64 DMMA product.
+ * RC_PREC_EMU64 (for condition numbers up to about 1e12, where a TF32/BF16 factor is too
+ * coarse for CG to converge): the factor is kept in FP64 storage and its trailing updates
+ * are exact int8 digit products on the tensor cores (7 signed 7-bit digits per entry below
+ * its row's largest, 28 digit-pair GEMMs with int32 accumulation, combined in FP64), within
+ * k 2^-44 of the row maxima per update of depth k; the diagonal blocks and panel solves are FP64 DMMA,
+ * and the preconditioner is applied in FP64. The outer panel width is at most 4096 (wider
+ * requests use 1024).
  * The call synchronises the stream (convergence is decided on the host). Returns
  * RC_ERR_NOT_CONVERGED when max_iter is reached first; d_info receives the failing pivot
  * when the low-precision factorisation breaks down (then X is not written). */
-enum { RC_PREC_TF32 = 0, RC_PREC_BF16 = 1 };
+enum { RC_PREC_TF32 = 0, RC_PREC_BF16 = 1, RC_PREC_EMU64 = 2 };
 typedef struct {
     double tol;          /* backward-error target (<= 0: 1e-15) */
     int max_iter;        /* CG iterations allowed in total (< 0: 100) */
@@ -318,6 +326,18 @@ int rc_syrk_tc(int precision, size_t n, size_t k, float alpha, const void* P, si
 enum { RC_SYRK_BESIDE = 1 };
 int rc_syrk_tc_ex(int precision, size_t n, size_t k, float alpha, const void* P, size_t ldp,
                   float beta, float* C, size_t ldc, int flags, void* stream);
+/* The trailing update of the RC_PREC_EMU64 factorisation as a standalone call: the lower
+ * triangle of the row-major n x n FP64 C <- alpha * P P^T + beta * C with P a row-major
+ * n x k FP64 matrix (k <= 16384), P split per row into 7 signed 7-bit digits below the
+ * row's largest |entry| and the 28 digit-pair products run as exact int8 GEMMs on the
+ * tcgen05 tensor cores (int32 accumulation), combined in FP64: every entry of P P^T is
+ * within k 2^-44 max_k |P(i, k)| max_k |P(j, k)| of the exact product (the digits truncate
+ * toward zero and the pairs of weight below 2^-56 are dropped). beta == 0 does not read C;
+ * the strictly upper triangle is not touched. Inf/NaN in a row of P gives NaN in its row
+ * and column of the product. (kernels::syrk<false>, include/remora/kernels/syrk.hpp:55-67,
+ * with emulated FP64 products.) */
+int rc_syrk_emu64(size_t n, size_t k, double alpha, const double* P, size_t ldp, double beta,
+                  double* C, size_t ldc, void* stream);
 /* Device workspace the solve caches for these sizes, in bytes. */
 int rc_spd_solve_mixed_workspace(int precision, size_t n, size_t nrhs,
                                  const rc_mixed_options* options, size_t* bytes);

@@ -15,6 +15,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libremora_cuda.so"
 RC_SUCCESS = 0
 RC_PREC_TF32 = 0
 RC_PREC_BF16 = 1
+RC_PREC_EMU64 = 2
 
 
 class MixedOptions(ctypes.Structure):
@@ -97,6 +98,7 @@ SIGNATURES: dict[str, list] = {
     "rc_spd_solve_mixed_workspace": [_I, _Z, _Z, _P, _P],
     "rc_syrk_tc": [_I, _Z, _Z, c_float, _P, _Z, c_float, _P, _Z, _P],
     "rc_syrk_tc_ex": [_I, _Z, _Z, c_float, _P, _Z, c_float, _P, _Z, _I, _P],
+    "rc_syrk_emu64": [_Z, _Z, c_double, _P, _Z, c_double, _P, _Z, _P],
     "rc_potrf_backward_f64": [_Z, _P, _Z, _P, _Z, _P, _Z, _P],
     "rc_trsm_backward_f64": [_I, _Z, _Z, _P, _Z, _P, _Z, _P, _Z, _P, _Z, _P],
     "rc_rbf_kernel_f64": [_Z, _I, _P, _P, c_double, _P, _Z, _P],

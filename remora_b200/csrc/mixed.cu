@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "assign.cuh"
+#include "emu64.cuh"
 #include "factor.cuh"
 #include "gemm.cuh"
 #include "mixed.cuh"
@@ -73,6 +74,36 @@ __global__ void __launch_bounds__(256) scale_to_f32_kernel(int64_t n, View<const
     }
 }
 
+// W64[i * ldw + j] = s_i A(i, j) s_j (+ theta on the diagonal) in FP64 for the lower
+// triangle, through a 32 x 33 tile as scale_to_f32_kernel (the working copy of the
+// factorisation whose trailing updates are digit products).
+__global__ void __launch_bounds__(256) scale_to_f64_kernel(int64_t n, View<const double> A, const double* s,
+                                                           double theta, double* W, int64_t ldw) {
+    __shared__ double tile[32][33];
+    const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
+    if (j0 > i0 + 31) return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < 32; r += 8) {
+        const int64_t i = i0 + tx, j = j0 + r;
+        double v = 0.0;
+        if (i < n && j < n && j <= i) v = s[i] * A(i, j) * s[j] + (i == j ? theta : 0.0);
+        tile[r][tx] = v;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int64_t i = i0 + r, j = j0 + tx;
+        if (i < n && j < n && j <= i) W[i * ldw + j] = tile[tx][r];
+    }
+}
+
+// Z[:, j] = s .* R[:, j] for the c columns (column-major, leading dimensions ldr, ldz).
+__global__ void col_scale_kernel(int64_t n, int64_t c, const double* s, const double* R, int64_t ldr, double* Z,
+                                 int64_t ldz) {
+    for (int64_t j = blockIdx.y; j < c; j += gridDim.y)
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            Z[i + j * ldz] = s[i] * R[i + j * ldr];
+}
+
 // The first pass over A when the CG products run on its int8 digit split: one read of
 // each 64-row x 128-column tile of column-major A (512 threads; a warp reads 64 rows of a
 // column, 16 bytes per lane when A allows) writes
@@ -95,7 +126,7 @@ __global__ void __launch_bounds__(kSplitThreads, 2) scale_split_kernel(int64_t n
     const int64_t tiles_x = (n + 127) / 128;
     const int64_t bx = blockIdx.x % tiles_x, i0 = (int64_t)(blockIdx.x / tiles_x) * kSplitRows;
     const int64_t jb = bx * 128, j0 = jb + w * 8;
-    const bool lower = jb <= i0 + kSplitRows - 1;
+    const bool lower = W != nullptr && jb <= i0 + kSplitRows - 1;  // W null: digits and row sums only
     const bool vec = (lda % 2 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0);
     double x[2][8];  // rows i0 + 2 lane + h, columns j0 + c
 #pragma unroll
@@ -643,26 +674,36 @@ static bool sliced_products(int64_t n, int64_t nrhs) { return nrhs <= 64 && n >=
 int mixed_workspace_bytes(int64_t n, int64_t nrhs, int prec, int outer, size_t* bytes) {
     const int64_t ldw = (n + 31) / 32 * 32;
     const int64_t nblk = (n + kNB - 1) / kNB;
-    const int64_t ow = outer > 0 ? outer : 1024;
+    // the panel width the solve uses (as normalised by spd_solve_mixed)
+    int64_t ow = (outer > 0 && outer % kNB == 0) ? outer : 1024;
+    if (prec == RC_PREC_EMU64 && ow > 4096) ow = 1024;
     size_t b = 0;
     auto add = [&](size_t x) { b += (x + 255) & ~size_t(255); };
-    add((size_t)n * ldw * sizeof(float));               // W
-    add((size_t)nblk * kNB * kNB * sizeof(float));      // diagonal-block inverses
-    if (prec == RC_PREC_BF16) {
-        add((size_t)n * ((ow + 63) / 64 * 64) * 2);  // BF16 outer panels (two)
-        add((size_t)n * ((ow + 63) / 64 * 64) * 2);
-        add((size_t)n * kNB * 2);                    // BF16 128-column block
+    if (prec == RC_PREC_EMU64) {
+        add((size_t)n * ldw * sizeof(double));           // W (FP64)
+        add((size_t)nblk * kNB * kNB * sizeof(double));  // diagonal-block inverses (FP64)
+        add(emu_panel_bytes(n, ow));                     // digit splits of two outer panels
+        add(emu_panel_bytes(n, ow));
+        add((size_t)kNB * nrhs * sizeof(double));        // TRSM tile buffer
+    } else {
+        add((size_t)n * ldw * sizeof(float));           // W
+        add((size_t)nblk * kNB * kNB * sizeof(float));  // diagonal-block inverses
+        if (prec == RC_PREC_BF16) {
+            add((size_t)n * ((ow + 63) / 64 * 64) * 2);  // BF16 outer panels (two)
+            add((size_t)n * ((ow + 63) / 64 * 64) * 2);
+            add((size_t)n * kNB * 2);                    // BF16 128-column block
+        }
+        const size_t chunked = (size_t)ldw * ((nrhs + RHS - 1) / RHS) * RHS;  // 64-column chunks, ld ldw
+        add(chunked * sizeof(float));                    // FP32 right-hand side of the preconditioner
+        add(chunked * sizeof(float));                    // FP32 intermediate of the preconditioner
+        add((size_t)ldw * 2 * RHS * sizeof(float));      // TF32 split of one solution block
+        add((size_t)kNB * nrhs * sizeof(float));         // TRSM tile buffer
+        add((size_t)((n + BS - 1) / BS) * BS * BS * sizeof(float));      // BS-block inverses
+        add((size_t)((n + BS - 1) / BS) * BS * BS / 2 * sizeof(float));  // their scratch
     }
     add((size_t)n * sizeof(double));                    // s
     add((size_t)n * sizeof(double));                    // column sums
     for (int i = 0; i < 4; ++i) add((size_t)n * nrhs * sizeof(double));  // R, Z, P, Q
-    const size_t chunked = (size_t)ldw * ((nrhs + RHS - 1) / RHS) * RHS;  // 64-column chunks, ld ldw
-    add(chunked * sizeof(float));                       // FP32 right-hand side of the preconditioner
-    add(chunked * sizeof(float));                       // FP32 intermediate of the preconditioner
-    add((size_t)ldw * 2 * RHS * sizeof(float));         // TF32 split of one solution block
-    add((size_t)kNB * nrhs * sizeof(float));            // TRSM tile buffer
-    add((size_t)((n + BS - 1) / BS) * BS * BS * sizeof(float));      // BS-block inverses
-    add((size_t)((n + BS - 1) / BS) * BS * BS / 2 * sizeof(float));  // their scratch
     add((size_t)8 * nrhs * sizeof(double));             // per-column scalars
     if (sliced_products(n, nrhs)) {
         add(ozaki_a_bytes(n, n));        // digit split of A
@@ -717,8 +758,103 @@ struct Mixed {
     void* oz_p = nullptr; // one sliced product's buffers
     bool use_oz = false;
     int* errw = nullptr;  // the library's device error word (a timed-out wait sets it)
+    // RC_PREC_EMU64: the FP64 working copy, its FP64 diagonal-block inverses (row-major),
+    // the digit splits of two outer panels and the TRSM tile buffer of the preconditioner.
+    double* W64 = nullptr;
+    double* Winv64 = nullptr;
+    void* Pe[2] = {nullptr, nullptr};
+    EmuPanel pe[2];
+    double* tmp64 = nullptr;
     View<const double> Av() const { return {A, 1, lda}; }
     View<float> Wv() const { return {W, ldw, 1}; }
+    View<double> W64v() const { return {W64, ldw, 1}; }
+
+    // The 128-column steps of one outer panel [k0, k0 + w) of the FP64 working copy, on
+    // stream st: factor (and invert, row-major) the diagonal block, solve the rows below it
+    // in place with that inverse on the 128 x 128 FP64 DMMA tile (one CTA owns every column
+    // of a row block), update the rest of the panel's columns in FP64.
+    int panel_chain64(int64_t k0, int64_t w, int* info, cudaStream_t st) {
+        const View<double> Wm = W64v();
+        for (int64_t j0 = k0; j0 < k0 + w; j0 += kNB) {
+            const int jb = (int)((k0 + w - j0) < kNB ? k0 + w - j0 : kNB);
+            double* Wb = Winv64 + (size_t)(j0 / kNB) * kNB * kNB;
+            RC_TRY(potrf_diag_block<double>(Wm.sub(j0, j0), jb, j0, Wb, true, info, st));
+            const int64_t rows = n - j0 - jb;
+            if (rows <= 0) continue;
+            const View<double> Pj = Wm.sub(j0 + jb, j0);
+            const View<const double> Pc = {Pj.p, Pj.rs, Pj.cs};
+            RC_TRY(gemm<double>(rows, jb, jb, 1.0, Pc, View<const double>{Wb, 1, kNB}, 0.0, Pj, kFull, 0, st, info));
+            const int64_t cw = k0 + w - (j0 + jb);
+            if (cw <= 0) continue;
+            RC_TRY(gemm<double>(rows, cw, jb, -1.0, Pc, Pc.t(), 1.0, Wm.sub(j0 + jb, j0 + jb), kLower, 0, st, info));
+        }
+        return RC_SUCCESS;
+    }
+
+    // The look-ahead schedule of factor() with an FP64 working copy: each factored outer
+    // panel is split into its int8 digits on the look-ahead stream, and T1 / T2 are digit-
+    // product updates (emu_update) instead of TF32/BF16 GEMMs. Panel p's split lives in
+    // Pe[p & 1]; the look-ahead stream has waited for T2(p - 2), its last reader, before it
+    // splits panel p (it waits for T2(p - 1) before T1(p), and T2(p - 2) ran before that).
+    int factor_emu(int outer, int* info) {
+        cudaStream_t la = lookahead_stream();
+        if (!la) return RC_ERR_CUDA;
+        cudaEvent_t ev_fork, ev_packed, ev_t2, ev_join;
+        if (cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_packed, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_t2, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess)
+            return RC_ERR_CUDA;
+        struct Events {
+            cudaEvent_t e[4];
+            ~Events() { for (cudaEvent_t x : e) cudaEventDestroy(x); }
+        } guard{{ev_fork, ev_packed, ev_t2, ev_join}};
+        auto ok = [](cudaError_t e) { return e == cudaSuccess ? RC_SUCCESS : RC_ERR_CUDA; };
+        RC_TRY(ok(cudaEventRecord(ev_fork, s)));
+        RC_TRY(ok(cudaStreamWaitEvent(la, ev_fork, 0)));
+        RC_TRY(panel_chain64(0, n < outer ? n : outer, info, la));
+        bool t2_pending = false;
+        for (int64_t p = 0, k0 = 0; k0 < n; ++p, k0 += outer) {
+            const int64_t w = (n - k0 < outer) ? n - k0 : outer;
+            const int64_t k1 = k0 + w, rows = n - k1;
+            if (rows <= 0) break;
+            EmuPanel& pn = pe[p & 1];
+            RC_TRY(emu_panel_layout(rows, w, Pe[p & 1], &pn));
+            RC_TRY(emu_slice_panel(pn, W64 + k1 * ldw + k0, ldw, la));
+            RC_TRY(ok(cudaEventRecord(ev_packed, la)));
+            if (t2_pending) RC_TRY(ok(cudaStreamWaitEvent(la, ev_t2, 0)));
+            const int64_t w1 = rows < outer ? rows : outer;  // width of panel p + 1
+            // T1: rows [k1, n) x columns [k1, k1 + w1) on the look-ahead stream
+            RC_TRY(emu_update(pn, 0, 0, rows, w1, -1.0, 1.0, W64 + k1 * ldw + k1, ldw, true, la, info));
+            // T2: rows and columns [k1 + w1, n) on the main stream
+            const int64_t r2 = rows - w1;
+            if (r2 > 0) {
+                RC_TRY(ok(cudaStreamWaitEvent(s, ev_packed, 0)));
+                RC_TRY(emu_update(pn, w1, w1, r2, r2, -1.0, 1.0, W64 + (k1 + w1) * ldw + (k1 + w1), ldw, true, s,
+                                  info));
+                RC_TRY(ok(cudaEventRecord(ev_t2, s)));
+                t2_pending = true;
+            } else {
+                t2_pending = false;
+            }
+            RC_TRY(panel_chain64(k1, w1, info, la));
+        }
+        RC_TRY(ok(cudaEventRecord(ev_join, la)));
+        return ok(cudaStreamWaitEvent(s, ev_join, 0));
+    }
+
+    // Zout = M^-1 Rin = S L^-T L^-1 S Rin, all in FP64, on st: block forward and backward
+    // substitution with the FP64 diagonal-block inverses (trsm_preinv) on the FP64 factor.
+    int precond_on64(const double* Rin, int64_t ldr, double* Zout, int64_t ldz, cudaStream_t st) {
+        const dim3 g = vec_grid(n, nrhs);
+        col_scale_kernel<<<g, 256, 0, st>>>(n, nrhs, sc, Rin, ldr, Zout, ldz);
+        RC_TRY(check_launch());
+        const View<const double> L = {W64, ldw, 1};
+        RC_TRY(trsm_preinv<double>(false, n, nrhs, L, Winv64, colmajor(Zout, ldz), tmp64, st));
+        RC_TRY(trsm_preinv<double>(true, n, nrhs, L, Winv64, colmajor(Zout, ldz), tmp64, st));
+        col_scale_kernel<<<g, 256, 0, st>>>(n, nrhs, sc, Zout, ldz, Zout, ldz);
+        return check_launch();
+    }
 
     // The 128-column steps of one outer panel [k0, k0 + w), on stream st: factor (and
     // invert) the diagonal block in FP64, solve the rows below it with that inverse on the
@@ -817,6 +953,7 @@ struct Mixed {
 
     // Zout = M^-1 Rin = S L^-T L^-1 S Rin (FP64 in/out, FP32 triangular solves), on st.
     int precond_on(const double* Rin, int64_t ldr, double* Zout, int64_t ldz, cudaStream_t st) {
+        if (W64) return precond_on64(Rin, ldr, Zout, ldz, st);
         const int64_t nch = (nrhs + RHS - 1) / RHS;  // 64-column chunks
         const dim3 g(ceil_div(n, 256) < 128u ? ceil_div(n, 256) : 128u, (unsigned)(nch * RHS));
         to_f32_scaled_kernel<<<g, 256, 0, st>>>(n, nrhs, sc, Rin, ldr, T32, ldv);
@@ -908,7 +1045,13 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     if (o.outer <= 0 || o.outer % kNB) o.outer = 1024;
     if (o.tol <= 0) o.tol = 1e-15;
     if (o.max_iter < 0) o.max_iter = 100;
-    const double uf = prec == RC_PREC_BF16 ? std::ldexp(1.0, -8) : std::ldexp(1.0, -11);
+    const bool emu = prec == RC_PREC_EMU64;
+    if (emu && o.outer > 4096) o.outer = 1024;  // int32 digit sums: K * 7 * 127^2 < 2^31
+    // u_f: the unit of the factor's trailing updates (about 2^-40 of the row maxima for
+    // the 7-digit products).
+    const double uf = prec == RC_PREC_BF16 ? std::ldexp(1.0, -8)
+                      : emu               ? std::ldexp(1.0, -40)
+                                          : std::ldexp(1.0, -11);
     // shift_factor < 0: adaptive -- theta = u_f / 4 first, then 2 and 16 u_f after a
     // breakdown of the low-precision factorisation. Measured CG steps at n = 16384 (TF32)
     // for theta = 0, u_f / 16, u_f / 4, u_f: kappa 1e2: 5, 5, 5, 6; kappa 1e4: 14, 14, 14,
@@ -934,25 +1077,35 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     M.n = n; M.nrhs = nrhs; M.prec = prec; M.s = s; M.A = A; M.lda = lda; M.errw = errw;
     M.ldw = (n + 31) / 32 * 32;
     M.nblk = (n + kNB - 1) / kNB;
-    M.W = buf.take<float>((size_t)n * M.ldw);
-    M.Winv = buf.take<float>((size_t)M.nblk * kNB * kNB);
+    M.ldv = (n + 31) / 32 * 32;
     M.ldpb = (o.outer + 63) / 64 * 64;
-    for (int q = 0; q < 2; ++q)
-        M.Pb[q] = prec == RC_PREC_BF16 ? static_cast<void*>(buf.take<uint16_t>((size_t)n * M.ldpb)) : nullptr;
-    M.Pi = prec == RC_PREC_BF16 ? static_cast<void*>(buf.take<uint16_t>((size_t)n * kNB)) : nullptr;
+    M.W = nullptr;
+    M.Winv = M.T32 = M.T32b = M.T32s = M.tmp = M.Y = M.Tinv = nullptr;
+    M.Pb[0] = M.Pb[1] = M.Pi = nullptr;
+    if (emu) {
+        M.W64 = buf.take<double>((size_t)n * M.ldw);
+        M.Winv64 = buf.take<double>((size_t)M.nblk * kNB * kNB);
+        for (int q = 0; q < 2; ++q) M.Pe[q] = buf.take<char>(emu_panel_bytes(n, o.outer));
+        M.tmp64 = buf.take<double>((size_t)kNB * nrhs);
+    } else {
+        M.W = buf.take<float>((size_t)n * M.ldw);
+        M.Winv = buf.take<float>((size_t)M.nblk * kNB * kNB);
+        for (int q = 0; q < 2; ++q)
+            M.Pb[q] = prec == RC_PREC_BF16 ? static_cast<void*>(buf.take<uint16_t>((size_t)n * M.ldpb)) : nullptr;
+        M.Pi = prec == RC_PREC_BF16 ? static_cast<void*>(buf.take<uint16_t>((size_t)n * kNB)) : nullptr;
+        M.T32 = buf.take<float>((size_t)M.ldv * ((nrhs + RHS - 1) / RHS) * RHS);
+        M.T32b = buf.take<float>((size_t)M.ldv * ((nrhs + RHS - 1) / RHS) * RHS);
+        M.T32s = buf.take<float>((size_t)M.ldv * 2 * RHS);
+        M.tmp = buf.take<float>((size_t)kNB * nrhs);
+        M.Y = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS);
+        M.Tinv = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS / 2);
+    }
     M.sc = buf.take<double>(n);
     M.colsum = buf.take<double>(n);
     M.R = buf.take<double>((size_t)n * nrhs);
     M.Z = buf.take<double>((size_t)n * nrhs);
     M.P = buf.take<double>((size_t)n * nrhs);
     M.Q = buf.take<double>((size_t)n * nrhs);
-    M.ldv = (n + 31) / 32 * 32;
-    M.T32 = buf.take<float>((size_t)M.ldv * ((nrhs + RHS - 1) / RHS) * RHS);
-    M.T32b = buf.take<float>((size_t)M.ldv * ((nrhs + RHS - 1) / RHS) * RHS);
-    M.T32s = buf.take<float>((size_t)M.ldv * 2 * RHS);
-    M.tmp = buf.take<float>((size_t)kNB * nrhs);
-    M.Y = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS);
-    M.Tinv = buf.take<float>((size_t)((n + BS - 1) / BS) * BS * BS / 2);
     M.dev_scalars = buf.take<double>((size_t)8 * nrhs);
     void* oz_a = nullptr;
     double* rsum = nullptr;
@@ -996,12 +1149,21 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
                 n, (n + 127) / 128, rsum, M.oz.Mp, M.colsum);
             RC_TRY(check_launch());
             M.use_oz = true;
+            if (emu) {
+                scale_to_f64_kernel<<<dim3(ceil_div(n, 32), ceil_div(n, 32)), 256, 0, s>>>(n, Av, M.sc, theta, M.W64,
+                                                                                          M.ldw);
+                RC_TRY(check_launch());
+            }
+        } else if (emu) {
+            scale_to_f64_kernel<<<dim3(ceil_div(n, 32), ceil_div(n, 32)), 256, 0, s>>>(n, Av, M.sc, theta, M.W64,
+                                                                                      M.ldw);
+            RC_TRY(check_launch());
         } else {
             scale_to_f32_kernel<<<dim3(ceil_div(n, 32), ceil_div(n, 32)), 256, 0, s>>>(n, Av, M.sc, theta, M.W,
                                                                                       M.ldw);
             RC_TRY(check_launch());
         }
-        RC_TRY(M.factor(o.outer, d_info));
+        RC_TRY(emu ? M.factor_emu(o.outer, d_info) : M.factor(o.outer, d_info));
         int h_err = 0;
         if (cudaMemcpyAsync(&h_info, d_info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaMemcpyAsync(&h_err, errw, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
@@ -1046,12 +1208,12 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
 
     // x0 = M^-1 b, after L^T is mirrored into W's upper triangle and the BS-block
     // inverses are built
-    {
+    if (!emu) {
         const unsigned nt = ceil_div(n, 32);
         mirror_lower_kernel<<<dim3(nt, nt), dim3(32, 8), 0, s>>>(n, M.W, M.ldw);
         RC_TRY(check_launch());
+        RC_TRY(build_block_inverses(n, M.W, M.ldw, M.Winv, M.Y, M.Tinv, s));
     }
-    RC_TRY(build_block_inverses(n, M.W, M.ldw, M.Winv, M.Y, M.Tinv, s));
     RC_TRY(M.precond(B, ldb, X, ldx));
     bool sliced = M.use_oz;  // CG products on the digit split until a convergence check fails
     std::vector<char> done(nrhs, 0);
@@ -1157,7 +1319,8 @@ extern "C" {
 int rc_spd_solve_mixed(int precision, size_t n, size_t nrhs, const double* A, size_t lda, const double* B, size_t ldb,
                        double* X, size_t ldx, const rc_mixed_options* options, int* d_info, rc_refine_info* info,
                        void* stream) {
-    if (precision != RC_PREC_TF32 && precision != RC_PREC_BF16) return RC_ERR_INVALID_ARGUMENT;
+    if (precision != RC_PREC_TF32 && precision != RC_PREC_BF16 && precision != RC_PREC_EMU64)
+        return RC_ERR_INVALID_ARGUMENT;
     if (!d_info) return RC_ERR_INVALID_ARGUMENT;
     if (n == 0 || nrhs == 0) return RC_SUCCESS;
     if (!A || !B || !X || lda < n || ldb < n || ldx < n) return RC_ERR_INVALID_ARGUMENT;

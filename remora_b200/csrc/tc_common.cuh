@@ -58,7 +58,7 @@ __device__ __forceinline__ int mbar_wait_bounded(uint64_t* bar, uint32_t parity,
 
 // Where a wait ran out (the second int of the error word): kernel * 100 + role * 10 + the
 // CTA's rank in its cluster.
-enum WaitKernel { kSiteTcGemm = 1, kSiteTcPair = 2, kSiteOzaki = 3, kSiteSelftest = 9 };
+enum WaitKernel { kSiteTcGemm = 1, kSiteTcPair = 2, kSiteOzaki = 3, kSiteEmu = 4, kSiteSelftest = 9 };
 enum WaitRole { kRoleProducer = 0, kRoleMma = 1, kRoleEpilogue = 2, kRoleDrain = 3 };
 
 // Stop this CTA's roles; on a timeout also record RC_ERR_TIMEOUT (and, for the first one on

@@ -205,9 +205,13 @@ def spd_solve_mixed(A: torch.Tensor, B: torch.Tensor, precision: str = "tf32", t
                     X: torch.Tensor | None = None):
     """Mixed-precision refined SPD solve (FP64 in/out; A full symmetric, column-major).
 
+    precision: "tf32" or "bf16" (a reduced-precision factor, for condition numbers up to
+    about 1e6..1e8) or "emu64" (an FP64 factor whose trailing updates are exact int8 digit
+    products, for condition numbers up to about 1e12).
+
     Returns (X, info dict, status) -- status 0 on convergence, 6 (RC_ERR_NOT_CONVERGED) when
     max_iter ran out; info["pivot"] is the failing pivot of a low-precision breakdown."""
-    from ._lib import RC_PREC_BF16, RC_PREC_TF32, MixedOptions, RefineInfo, lib
+    from ._lib import RC_PREC_BF16, RC_PREC_EMU64, RC_PREC_TF32, MixedOptions, RefineInfo, lib
     if A.dtype != torch.float64 or B.dtype != torch.float64:
         raise TypeError("spd_solve_mixed takes FP64 matrices")
     n = A.shape[0]
@@ -218,7 +222,7 @@ def spd_solve_mixed(A: torch.Tensor, B: torch.Tensor, precision: str = "tf32", t
     if X is None:
         X = torch.empty((B.shape[1], n), dtype=torch.float64, device=B.device).t()
     tx, ldx = layout(X)
-    prec = {"tf32": RC_PREC_TF32, "bf16": RC_PREC_BF16}[precision]
+    prec = {"tf32": RC_PREC_TF32, "bf16": RC_PREC_BF16, "emu64": RC_PREC_EMU64}[precision]
     opts = MixedOptions(tol, max_iter, outer, shift_factor)
     info = RefineInfo()
     d_info = torch.zeros(1, dtype=torch.int32, device=A.device)
