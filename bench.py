@@ -462,6 +462,13 @@ def run_case(args) -> None:
         for _ in range(reps):
             _lib.call("rc_syrk_tc", 1 if args.precision == "bf16" else 0, n, k, -1.0, ctypes.c_void_p(P.data_ptr()),
                       k, 1.0, ctypes.c_void_p(C.data_ptr()), n, sptr)
+    elif args.case == "syrk_emu":  # the emulated-FP64 trailing update, n x n lower, depth 1024
+        n, k = 8192, 1024
+        P = torch.randn((n, k), device=dev, dtype=torch.float64)
+        C = torch.zeros((n, n), device=dev, dtype=torch.float64)
+        for _ in range(reps):
+            _lib.call("rc_syrk_emu64", n, k, -1.0, ctypes.c_void_p(P.data_ptr()), k, 1.0,
+                      ctypes.c_void_p(C.data_ptr()), n, sptr)
     elif args.case == "dgemm":  # FP64 DMMA GEMM 4096^3
         n = 4096
         A = torch.rand((n, n), device=dev, dtype=torch.float64)
@@ -526,7 +533,7 @@ def main() -> None:
     ap.add_argument("--ref-n", type=int, default=4096, help="CPU reference sample size")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--case", choices=["syrk_tc", "dgemm", "potrf", "rng", "mixed", "batched", "sliced"],
+    ap.add_argument("--case", choices=["syrk_tc", "syrk_emu", "dgemm", "potrf", "rng", "mixed", "batched", "sliced"],
                     help="run one small kernel case (for ncu captures) instead of the benchmark")
     ap.add_argument("--watchdog", type=float, default=600.0,
                     help="seconds after which a run that has not finished exits with status 3")

@@ -13,7 +13,8 @@
 // (7 * 127^2 * K < 2^31 for K <= 16384). One tcgen05.mma of slice t against the stacked
 // slices [a_1 .. a_(8-t)] of the 64 B rows lands in the accumulators d = t+1 .. 8 side by
 // side in TMEM (7 x 64 columns), as in the right-hand-side products of ozaki.cu; the
-// epilogue combines the seven int32 accumulators in FP64 (Horner) and adds
+// epilogue combines the seven int32 accumulators (two exact int64 partial sums, one FP64
+// rounding) and adds
 // alpha 2^(e_i + e_j - 14) times the result into C. Each product term then misses the pairs
 // of weight 2^-63 and below and the truncated remainders: at most 2^-46 2^(e_i + e_j), so
 // an update of depth K is within K 2^-46 2^(e_i + e_j) <= K 2^-44 m_i m_j (m_i the row's
@@ -21,9 +22,12 @@
 // within reach of FP64 refinement for condition numbers up to ~1e12.
 //
 // Per CTA: a 128-row x 64-column tile of C. Warp 0 streams, per 128-wide K block, the
-// seven 128-row slices of the A rows through a 6-deep ring and the seven 64-row slices of
+// seven 128-row slices of the A rows through a 7-deep ring and the seven 64-row slices of
 // the B rows (one 3-D TMA box) through a 2-deep ring; warp 1 issues the MMAs; warps 2..5
-// finish the tile. Every mbarrier wait is bounded, as in the other tensor-core kernels.
+// finish the tile: during the main loop they pull their rows of the C tile into L2, then
+// combine the accumulators into a staging tile in the (by then idle) A ring and update C a
+// row at a time across the lanes, so that every C access is coalesced. Every mbarrier wait
+// is bounded, as in the other tensor-core kernels.
 #include <climits>
 #include <cudaTypedefs.h>
 
@@ -38,11 +42,14 @@ namespace {
 using namespace tc;
 constexpr int S = kEmuSlices;
 constexpr int EMU_THREADS = 192;
-constexpr int A_STAGES = 6;
+constexpr int A_STAGES = 7;
 constexpr int A_TILE = 128 * 128;     // one slice of 128 rows x 128 bytes
 constexpr int B_TILE = 64 * 128 * S;  // all slices of 64 rows x 128 bytes
 constexpr size_t EMU_SMEM = 1024 + (size_t)A_STAGES * A_TILE + 2 * (size_t)B_TILE + 256;
 static_assert(EMU_SMEM <= 232448, "shared memory of the digit-product update");
+// The epilogue's staging tile (128 rows x 64 FP64 values, rows padded to 65) reuses the A ring.
+constexpr int kStageLd = 65;
+static_assert(128 * kStageLd * 8 <= A_STAGES * A_TILE, "staging tile");
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 int64_t round_up(int64_t x, int64_t q) { return (x + q - 1) / q * q; }
@@ -96,6 +103,51 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, ui
             "r"(smem_u32(dst)),
         "l"(tm), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
         : "memory");
+}
+
+// 16 int32 accumulator columns of this warp's TMEM lanes, without waiting (tmem_wait_ld).
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Shared-space accesses of the staging tile (explicitly .shared, so that the compiler and the
+// memory pipeline never order them behind the epilogue's global loads and stores).
+__device__ __forceinline__ void sts_f64(uint32_t addr, double v) {
+    asm volatile("st.shared.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
+}
+__device__ __forceinline__ double lds_f64(uint32_t addr) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr) : "memory");
+    return v;
+}
+
+// 2^e as a double for e in [-1022, 1023] (the exponent field alone).
+__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
+// h * 2^e, correctly rounded (as ldexp(h, e)), for |h| in {0} u [2^-42, 2^35) (a
+// combination of the seven accumulators), without a branch: e is clamped to [-2044, 2044]
+// (beyond it the result is 0 or Inf either way) and split into halves e1 + e2, both within
+// the normal exponents; h 2^e1 is then exact (normal, |e1| <= 1022 keeps it far from
+// overflow, and it is subnormal only when the final result rounds to zero), so the second
+// product is the one rounding.
+__device__ __forceinline__ double scale_pow2(double h, int e) {
+    e = max(-2044, min(e, 2044));
+    const int e1 = e >> 1;
+    return (h * pow2(e1)) * pow2(e - e1);
+}
+
+// The seven int32 accumulators v[0] (weight 1) .. v[6] (weight 2^-42) as one FP64 value:
+// v0 2^21 + v1 2^14 + v2 2^7 + v3 and v4 2^14 + v5 2^7 + v6 are exact in int64 (|v| < 2^31),
+// and exact in FP64 (below 2^53 and 2^46), so h has one rounding.
+__device__ __forceinline__ double combine7(const uint32_t (&v)[S][16], int x) {
+    const long long hi = ((((long long)(int)v[0][x] * 128 + (int)v[1][x]) * 128 + (int)v[2][x]) * 128) + (int)v[3][x];
+    const long long lo = ((long long)(int)v[4][x] * 128 + (int)v[5][x]) * 128 + (int)v[6][x];
+    return fma((double)hi, 0x1p-21, (double)lo * 0x1p-42);
 }
 
 // C(i, j) <- alpha * (P_A P_B^T)(i, j) + beta * C(i, j) on one 128 x 64 tile (see the file
@@ -233,38 +285,73 @@ __global__ void __launch_bounds__(EMU_THREADS, 1)
             }
         }
     } else {
-        const int q = warp & 3;  // TMEM lane quadrant this warp may access
+        // Epilogue warps: warp w owns TMEM lanes 32 (w % 4) .. and the same 32 rows of the tile.
+        const int q = warp & 3;
+        const int r0 = 32 * q;
+        const int64_t i = i0 + r0 + lane;  // the row whose accumulators this thread reads
+        const int ei = i < M ? rexp[a0 + i] : 0;
+        if (i < M && beta != 0.0) {  // while the main loop runs: this row of the C tile into L2
+            const double* crow = C + i * ldc + j0;
+            const int64_t cols = N - j0 < 64 ? N - j0 : 64;
+            for (int64_t c = 0; c < cols; c += 16) asm volatile("prefetch.global.L2 [%0];" ::"l"(crow + c));
+        }
         const int w = mbar_wait_bounded(done, 0, stop, err, abort, limit_ns);
         const bool ok = w == kWaitOk;
         if (!ok) raise_stop(stop, err, w, kSiteEmu * 100 + kRoleEpilogue * 10);
         tc_fence_after();
         if (__all_sync(0xffffffffu, ok && !*stop)) {
-            const int64_t i = i0 + 32 * q + lane;
-            const bool row_ok = i < M;
-            const int ei = row_ok ? rexp[a0 + i] : 0;
-            double* crow = C + i * ldc;
+            // 1. The seven accumulators of this thread's row, combined into this warp's 32 rows of a staging tile in the operand ring, idle now that
+            //    every load has been consumed and every MMA has completed.
+            const uint32_t stage = smem_u32(sA) + (uint32_t)(r0 * kStageLd * 8);
+            const uint32_t srow = stage + (uint32_t)(lane * kStageLd * 8);
 #pragma unroll 1
             for (int cc = 0; cc < 64; cc += 16) {
-                double h[16];
+                uint32_t v[S][16];
 #pragma unroll
-                for (int x = 0; x < 16; ++x) h[x] = 0.0;
+                for (int d = 0; d < S; ++d) tmem_ld16_async(tmem + ((uint32_t)r0 << 16) + (uint32_t)(64 * d + cc), v[d]);
+                tmem_wait_ld();
+#pragma unroll
+                for (int x = 0; x < 16; ++x) sts_f64(srow + (uint32_t)((cc + x) * 8), combine7(v, x));
+            }
+            __syncwarp();
+            // 2. The warp's 32 rows of C, a row at a time across the lanes (columns lane and
+            //    lane + 32): every C load of the 32 rows in flight at once, then the updates.
+            //    Tile-local indices: row rl = r0 + rr, column cl = lane + 32 u; C(rl, cl) is
+            //    written when rl < mrem, cl < nrem and, for the lower triangle, cl - rl <= dlim.
+            const int mrem = (int)(M - i0 < 128 ? M - i0 : 128), nrem = (int)(N - j0 < 64 ? N - j0 : 64);
+            const int dlim = lower ? (int)(i0 - j0 < 256 ? i0 - j0 : 256) : 256;
+            const bool rd = beta != 0.0;
+            int ej[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) ej[u] = lane + 32 * u < nrem ? rexp[b0 + j0 + lane + 32 * u] : 0;
+            double* cw = C + (i0 + r0) * ldc + j0 + lane;  // this lane's column of the warp's first row
 #pragma unroll 1
-                for (int d = S - 1; d >= 0; --d) {  // Horner from the lightest accumulator
-                    int v[16];
-                    tmem_ld16i(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(64 * d + cc), v);
+            for (int half = 0; half < 32; half += 16) {
+                double cv[16][2], hv[16][2];
 #pragma unroll
-                    for (int x = 0; x < 16; ++x) h[x] = fma(h[x], 0.0078125, (double)v[x]);
+                for (int rr = 0; rr < 16; ++rr) {
+                    const int rl = r0 + half + rr;
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const int cl = lane + 32 * u;
+                        const bool live = rl < mrem && cl < nrem && cl - rl <= dlim;
+                        cv[rr][u] = (live && rd) ? cw[(int64_t)(half + rr) * ldc + 32 * u] : 0.0;
+                        hv[rr][u] = lds_f64(stage + (uint32_t)(((half + rr) * kStageLd + cl) * 8));
+                    }
                 }
-                if (!row_ok) continue;
 #pragma unroll
-                for (int x = 0; x < 16; ++x) {
-                    const int64_t j = j0 + cc + x;
-                    if (j >= N || (lower && j > i)) continue;
-                    const int ej = rexp[b0 + j];
-                    const double val = (ei == kOzBadExp || ej == kOzBadExp)
-                                           ? __longlong_as_double(0x7FF8000000000000ll)
-                                           : ldexp(h[x], ei + ej - 14);
-                    crow[j] = beta == 0.0 ? alpha * val : fma(alpha, val, beta * crow[j]);
+                for (int rr = 0; rr < 16; ++rr) {
+                    const int rl = r0 + half + rr;
+                    const int er = __shfl_sync(0xffffffffu, ei, half + rr);
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const int cl = lane + 32 * u;
+                        const bool bad = er == kOzBadExp || ej[u] == kOzBadExp;
+                        double val = scale_pow2(hv[rr][u], bad ? 0 : er + ej[u] - 14);
+                        val = bad ? __longlong_as_double(0x7FF8000000000000ll) : val;
+                        const double out = rd ? fma(alpha, val, beta * cv[rr][u]) : alpha * val;
+                        if (rl < mrem && cl < nrem && cl - rl <= dlim) cw[(int64_t)(half + rr) * ldc + 32 * u] = out;
+                    }
                 }
             }
         }
