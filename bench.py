@@ -353,6 +353,40 @@ def run_ours(args) -> None:
     else:
         del A
 
+    # kappa = 1e10 beside the headline: a TF32/BF16 factor cannot precondition it to FP64
+    # accuracy, so the solve runs with the emulated-FP64 factor ("emu64": int8 digit-product
+    # trailing updates), against cuSOLVER's FP64 Cholesky solve on the same system.
+    k10 = None
+    if not args.no_kappa10 and world == 1:
+        phase("kappa 1e10 (emu64 factor)")
+        A10 = make_spd(n, 1e10, seed=4321, device=dev)
+        X10 = torch.empty((nrhs, n), device=dev, dtype=torch.float64).t()
+        st10, info10 = 0, {}
+        for i in range(2):  # one warm-up solve, one timed
+            torch.cuda.synchronize()
+            e0.record(stream)
+            _, info10, st10 = ops.spd_solve_mixed(A10, B, "emu64", tol=1e-15, max_iter=args.max_iter, X=X10)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            fail_on_status(lib, st10, info10, f"kappa 1e10 solve {i}")
+        t10 = e0.elapsed_time(e1) / 1e3
+        bwd10 = backward_error(A10, X10, B)
+        del X10
+        e0.record(stream)
+        L, _ = torch.linalg.cholesky_ex(A10)
+        Xc = torch.cholesky_solve(B, L)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tc10 = e0.elapsed_time(e1) / 1e3
+        cbwd10 = backward_error(A10, Xc, B)
+        del L, Xc, A10
+        torch.cuda.empty_cache()
+        k10 = {"kappa": 1e10, "precision": "emu64", "ms": t10 * 1e3, "tflops": flops(n, nrhs) / t10 / 1e12,
+               "backward_error": bwd10, "converged": info10.get("converged"), "cg_iterations": info10.get("iterations"),
+               "factor_ms": info10.get("factor_ms"), "refine_ms": info10.get("refine_ms"),
+               "cusolver_ms": tc10 * 1e3, "cusolver_backward_error": cbwd10,
+               "speedup_vs_cusolver": tc10 / t10, "speedup_vs_fp64_plain": t64 / t10}
+
     phase("roofline kernel")
     # Roofline: the dominant kernel, the tcgen05 trailing update (lower SYRK C -= P P^T)
     # at the largest trailing shape of the factorisation, timed with CUDA events on its own
@@ -394,6 +428,35 @@ def run_ours(args) -> None:
     del P, C
     torch.cuda.empty_cache()
 
+    # The emulated-FP64 trailing update (the kappa = 1e10 path's dominant kernel) at the same
+    # shape: FP64 P and C, 28 int8 digit-pair products per FP64 product.
+    P64 = torch.randn((rows, outer), device=dev, dtype=torch.float64)
+    C64 = torch.zeros((rows, rows), device=dev, dtype=torch.float64)
+
+    def syrk_emu():
+        _lib.call("rc_syrk_emu64", rows, outer, -1.0, ctypes.c_void_p(P64.data_ptr()), outer, 1.0,
+                  ctypes.c_void_p(C64.data_ptr()), rows, sptr)
+    for _ in range(2):
+        syrk_emu()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(5):
+        syrk_emu()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_emu = e0.elapsed_time(e1) / 1e3 / 5
+    del P64, C64
+    torch.cuda.empty_cache()
+    int8_peak = 2.0 * peaks["bf16_tflops"]
+    emu_roof = {"kernel": f"emu_update_kernel (tcgen05 kind::i8, lower SYRK {rows}x{rows}x{outer} in emulated FP64, "
+                          "7 digits, 28 digit-pair products)",
+                "bound": "tensor", "achieved": 28 * syrk_flops / t_emu / 1e12, "peak": int8_peak, "unit": "TOPS (int8)",
+                "frac": 28 * syrk_flops / t_emu / 1e12 / int8_peak, "traffic": None,
+                "fp64_equivalent_tflops": syrk_flops / t_emu / 1e12, "ms": t_emu * 1e3,
+                "peak_source": "2 x bf16_tflops (the int8 rate is twice the bf16 rate) of "
+                               + peaks.get("source", "?") + " peaks",
+                "algorithmic": "28 n(n+1)k int8 operations per launch"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         phase("CPU reference sample")
@@ -430,9 +493,11 @@ def run_ours(args) -> None:
                          "peak_source": ("bf16_tflops of " if prec else "bf16_tflops/2 (TF32 rate) of ")
                          + peaks.get("source", "?") + " peaks",
                          "algorithmic": "n(n+1)k flops per launch"},
+            "roofline_emu64": emu_roof,
             "roofline_alone": {"kernel": "the same kernel in the deeper-ring configuration of a lone rc_syrk_tc call",
                                "achieved": achieved_alone, "peak": peak, "unit": "TFLOP/s",
                                "frac": achieved_alone / peak},
+            "kappa_1e10": k10,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),
@@ -528,10 +593,11 @@ def main() -> None:
     ap.add_argument("--n", type=int, default=32768)
     ap.add_argument("--nrhs", type=int, default=64)
     ap.add_argument("--kappa", type=float, default=1e2)
-    ap.add_argument("--precision", choices=["tf32", "bf16"], default="tf32")
+    ap.add_argument("--precision", choices=["tf32", "bf16", "emu64"], default="tf32")
     ap.add_argument("--max-iter", type=int, default=200)
     ap.add_argument("--ref-n", type=int, default=4096, help="CPU reference sample size")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-kappa10", action="store_true", help="skip the kappa = 1e10 emu64 solve beside the headline")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--case", choices=["syrk_tc", "syrk_emu", "dgemm", "potrf", "rng", "mixed", "batched", "sliced"],
                     help="run one small kernel case (for ncu captures) instead of the benchmark")

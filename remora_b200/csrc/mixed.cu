@@ -28,6 +28,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 #include <vector>
 
 #include "assign.cuh"
@@ -967,41 +968,17 @@ struct Mixed {
         from_f32_scaled_kernel<<<dim3(g.x, (unsigned)nrhs), 256, 0, st>>>(n, nrhs, sc, T32, ldv, Zout, ldz);
         return check_launch();
     }
-    int precond(const double* Rin, int64_t ldr, double* Zout, int64_t ldz) {
-        return precond_on(Rin, ldr, Zout, ldz, s);
-    }
 
     // The CG preconditioner R -> Z is replayed as one CUDA graph: its ~6 n/128 small
-    // launches per application would otherwise be bound by launch latency.
+    // launches per application would otherwise be bound by launch latency. Every buffer it
+    // touches lies in the solve's workspace, so the instantiated graph is kept for later
+    // solves with the same workspace, sizes and precision (g_graphs).
+    const void* ws_base = nullptr;
+    size_t ws_bytes = 0;
+    int outer = 0;
     cudaGraphExec_t graph_exec = nullptr;
     size_t graph_kernels = 0;
-    int precond_RZ() {
-        if (!graph_exec) {
-            cudaStream_t cs;
-            if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return RC_ERR_CUDA;
-            const unsigned long long before = rc_launch_count();
-            cudaGraph_t graph = nullptr;
-            int st = RC_SUCCESS;
-            if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed) != cudaSuccess) st = RC_ERR_CUDA;
-            if (st == RC_SUCCESS) st = precond_on(R, n, Z, n, cs);
-            if (cudaStreamEndCapture(cs, &graph) != cudaSuccess && st == RC_SUCCESS) st = RC_ERR_CUDA;
-            cudaStreamDestroy(cs);
-            graph_kernels = (size_t)(rc_launch_count() - before);
-            if (st == RC_SUCCESS && cudaGraphInstantiate(&graph_exec, graph, 0) != cudaSuccess) st = RC_ERR_CUDA;
-            if (graph) cudaGraphDestroy(graph);
-            if (st != RC_SUCCESS) {
-                cudaGetLastError();
-                graph_exec = nullptr;
-                return st;
-            }
-        }
-        if (cudaGraphLaunch(graph_exec, s) != cudaSuccess) return RC_ERR_CUDA;
-        for (size_t i = 0; i < graph_kernels; ++i) count_launch();
-        return RC_SUCCESS;
-    }
-    ~Mixed() {
-        if (graph_exec) cudaGraphExecDestroy(graph_exec);
-    }
+    int precond_RZ();
 
     // Rout = B - A X: FP64 DMMA, or (sliced) on the int8 digit split of A.
     int residual(const double* B, int64_t ldb, const double* X, int64_t ldx, double* Rout, bool sliced = false) {
@@ -1030,6 +1007,71 @@ struct Mixed {
                    : RC_ERR_CUDA;
     }
 };
+
+// Instantiated preconditioner graphs, one per (device, workspace address), valid for the
+// key it was built from: the workspace size (all buffers are carved from it in a fixed
+// layout), the sizes, the precision, the panel width and the wait limit of the tensor-core
+// kernels. A workspace belongs to one stream, whose calls are ordered, so a graph that a
+// new key replaces ran last on the calling stream.
+struct PrecondGraph {
+    int dev;
+    const void* base;
+    size_t bytes;
+    int64_t n, nrhs;
+    int prec, outer;
+    uint64_t limit_ns;
+    cudaGraphExec_t exec;
+    size_t kernels;
+};
+std::mutex g_graph_mutex;
+std::vector<PrecondGraph> g_graphs;
+
+int Mixed::precond_RZ() {
+    if (!graph_exec) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return RC_ERR_CUDA;
+        const uint64_t lim = wait_limit_ns();
+        std::lock_guard<std::mutex> lock(g_graph_mutex);
+        PrecondGraph* slot = nullptr;
+        for (PrecondGraph& g : g_graphs)
+            if (g.dev == dev && g.base == ws_base) slot = &g;
+        if (slot && slot->bytes == ws_bytes && slot->n == n && slot->nrhs == nrhs && slot->prec == prec &&
+            slot->outer == outer && slot->limit_ns == lim) {
+            graph_exec = slot->exec;
+            graph_kernels = slot->kernels;
+        } else {
+            cudaStream_t cs;
+            if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return RC_ERR_CUDA;
+            const unsigned long long before = rc_launch_count();
+            cudaGraph_t gr = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            int st = RC_SUCCESS;
+            if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed) != cudaSuccess) st = RC_ERR_CUDA;
+            if (st == RC_SUCCESS) st = precond_on(R, n, Z, n, cs);
+            if (cudaStreamEndCapture(cs, &gr) != cudaSuccess && st == RC_SUCCESS) st = RC_ERR_CUDA;
+            cudaStreamDestroy(cs);
+            const size_t kernels = (size_t)(rc_launch_count() - before);
+            if (st == RC_SUCCESS && cudaGraphInstantiate(&exec, gr, 0) != cudaSuccess) st = RC_ERR_CUDA;
+            if (gr) cudaGraphDestroy(gr);
+            if (st != RC_SUCCESS) {
+                cudaGetLastError();
+                return st;
+            }
+            if (slot) {
+                if (cudaStreamSynchronize(s) != cudaSuccess) return RC_ERR_CUDA;
+                cudaGraphExecDestroy(slot->exec);
+                *slot = {dev, ws_base, ws_bytes, n, nrhs, prec, outer, lim, exec, kernels};
+            } else {
+                g_graphs.push_back({dev, ws_base, ws_bytes, n, nrhs, prec, outer, lim, exec, kernels});
+            }
+            graph_exec = exec;
+            graph_kernels = kernels;
+        }
+    }
+    if (cudaGraphLaunch(graph_exec, s) != cudaSuccess) return RC_ERR_CUDA;
+    for (size_t i = 0; i < graph_kernels; ++i) count_launch();
+    return RC_SUCCESS;
+}
 
 }  // namespace
 
@@ -1074,6 +1116,9 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
     if (!base) return RC_ERR_ALLOC;
     Buf buf{base};
     Mixed M;
+    M.ws_base = base;
+    M.ws_bytes = bytes;
+    M.outer = o.outer;
     M.n = n; M.nrhs = nrhs; M.prec = prec; M.s = s; M.A = A; M.lda = lda; M.errw = errw;
     M.ldw = (n + 31) / 32 * 32;
     M.nblk = (n + kNB - 1) / kNB;
@@ -1214,7 +1259,11 @@ int spd_solve_mixed(int prec, int64_t n, int64_t nrhs, const double* A, int64_t 
         RC_TRY(check_launch());
         RC_TRY(build_block_inverses(n, M.W, M.ldw, M.Winv, M.Y, M.Tinv, s));
     }
-    RC_TRY(M.precond(B, ldb, X, ldx));
+    // x0 = M^-1 B through the same CUDA graph as the CG steps (R = B, Z = M^-1 R, X = Z):
+    // the FP64 preconditioner of RC_PREC_EMU64 is ~6 n / 128 launches.
+    RC_TRY(copy2d<double, double>(n, nrhs, 1.0, View<const double>{B, 1, ldb}, colmajor(M.R, n), s));
+    RC_TRY(M.precond_RZ());
+    RC_TRY(copy2d<double, double>(n, nrhs, 1.0, View<const double>{M.Z, 1, n}, View<double>{X, 1, ldx}, s));
     bool sliced = M.use_oz;  // CG products on the digit split until a convergence check fails
     std::vector<char> done(nrhs, 0);
     int iters = 0, residuals = 0;
