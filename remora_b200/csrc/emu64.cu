@@ -241,40 +241,52 @@ __global__ void __launch_bounds__(EMU_THREADS, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            int a_used = 0;
-            for (int kb = 0; kb < KB && !*stop; ++kb) {
+            // The tensor pipe idles through every instruction this thread runs between two
+            // MMAs (its queue is shallow: a pause after a slice's MMAs shows up one for one in
+            // the main loop), so the slices are unrolled with their descriptors, shapes and
+            // accumulator columns fixed at compile time: A stage t always holds slice t and is
+            // filled once per K block (phase parity kb & 1).
+            static_assert(A_STAGES == S, "one A stage per slice");
+            uint64_t adesc[S];
+#pragma unroll
+            for (int t = 0; t < S; ++t) adesc[t] = sw128_kmajor_desc(sA + t * A_TILE);
+            const uint64_t b0d0 = sw128_kmajor_desc(sB), b0d1 = sw128_kmajor_desc(sB + 256 * 128);
+            const uint64_t b1d0 = sw128_kmajor_desc(sB + B_TILE), b1d1 = sw128_kmajor_desc(sB + B_TILE + 256 * 128);
+            bool ok = true;
+            for (int kb = 0; kb < KB && ok; ++kb) {
                 const int bs = kb & 1;
-                const int w = mbar_wait_bounded(&bfull[bs], (kb >> 1) & 1, stop, err, abort, limit_ns);
+                const uint32_t par = (uint32_t)kb & 1u;
+                int w = mbar_wait_bounded(&bfull[bs], (kb >> 1) & 1, stop, err, abort, limit_ns);
                 if (w != kWaitOk) {
                     raise_stop(stop, err, w, kSiteEmu * 100 + kRoleMma * 10);
                     break;
                 }
                 tc_fence_after();
-                const uint64_t bd0 = sw128_kmajor_desc(sB + bs * B_TILE);
-                const uint64_t bd1 = sw128_kmajor_desc(sB + bs * B_TILE + 256 * 128);
+                const uint64_t bd0 = bs ? b1d0 : b0d0, bd1 = bs ? b1d1 : b0d1;
+#pragma unroll
                 for (int t = 0; t < S; ++t) {
-                    const int as = a_used % A_STAGES;
-                    const int wa = mbar_wait_bounded(&afull[as], (a_used / A_STAGES) & 1, stop, err, abort, limit_ns);
-                    if (wa != kWaitOk) {
-                        raise_stop(stop, err, wa, kSiteEmu * 100 + kRoleMma * 10);
+                    w = mbar_wait_bounded(&afull[t], par, stop, err, abort, limit_ns);
+                    if (w != kWaitOk) {
+                        raise_stop(stop, err, w, kSiteEmu * 100 + kRoleMma * 10);
+                        ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint64_t ad = sw128_kmajor_desc(sA + as * A_TILE);
                     // a_t x [b_1 .. b_(S-t)] -> accumulators d = t .. S-1 (columns 64 t ..)
-                    const int n_all = 64 * (S - t);
+                    constexpr int kCols = 64;
+                    const int n_all = kCols * (S - t);
                     const int n1 = n_all < 256 ? n_all : 256;
-                    const uint32_t col = (uint32_t)(64 * t);
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk) {
                         const uint32_t acc = (kb | t | kk) != 0 ? 1u : 0u;
-                        umma_i8(tmem + col, ad + 2 * kk, bd0 + 2 * kk, i8_idesc(n1), acc);
-                        if (n_all > 256) umma_i8(tmem + col + 256, ad + 2 * kk, bd1 + 2 * kk, i8_idesc(n_all - 256), acc);
+                        umma_i8(tmem + (uint32_t)(kCols * t), adesc[t] + 2 * kk, bd0 + 2 * kk, i8_idesc(n1), acc);
+                        if (n_all > 256)
+                            umma_i8(tmem + (uint32_t)(kCols * t + 256), adesc[t] + 2 * kk, bd1 + 2 * kk,
+                                    i8_idesc(n_all - 256), acc);
                     }
-                    umma_commit(&aempty[as]);
-                    ++a_used;
+                    umma_commit(&aempty[t]);
                 }
-                umma_commit(&bempty[bs]);
+                if (ok) umma_commit(&bempty[bs]);
             }
             umma_commit(done);
             if (*stop) {
