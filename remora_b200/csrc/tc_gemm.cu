@@ -125,21 +125,29 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
             const uint32_t fmt = BF16 ? 1u : 2u;
             const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(BN >> 3) << 17) |
                                    ((uint32_t)(128 >> 4) << 24);
+            // The tensor pipe idles through every instruction this thread runs between two
+            // MMAs: the ring position is carried incrementally and the descriptors advance by
+            // a fixed stride.
+            const uint64_t ad0 = sw128_kmajor_desc(sA), bd0 = sw128_kmajor_desc(sB);
+            constexpr uint64_t kAStep = Cfg::A_BYTES >> 4, kBStep = Cfg::B_BYTES >> 4;
+            int s = 0;
+            uint32_t ph = 0;
             for (int kb = 0; kb < KB; ++kb) {
-                const int s = kb % STAGES;
-                const uint32_t ph = (kb / STAGES) & 1;
                 const int w = mbar_wait_bounded(&full[s], ph, stop, err, abort, limit_ns);
                 if (w != kWaitOk) {
                     raise_stop(stop, err, w, kSiteTcGemm * 100 + kRoleMma * 10);
                     break;
                 }
                 tc_fence_after();
-                const uint64_t ad = sw128_kmajor_desc(sA + s * Cfg::A_BYTES);
-                const uint64_t bd = sw128_kmajor_desc(sB + s * Cfg::B_BYTES);
+                const uint64_t ad = ad0 + (uint64_t)s * kAStep, bd = bd0 + (uint64_t)s * kBStep;
 #pragma unroll
                 for (int kk = 0; kk < MMAS_PER_STAGE; ++kk)
                     umma<BF16>(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
                 umma_commit(&empty[s]);
+                if (++s == STAGES) {
+                    s = 0;
+                    ph ^= 1u;
+                }
             }
             umma_commit(done);
         }
@@ -412,7 +420,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
             const uint32_t fmt = BF16 ? 1u : 2u;
             const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(256 >> 3) << 17) |
                                    ((uint32_t)(256 >> 4) << 24);
-            int64_t g = 0;
+            // The tensor pipe idles through every instruction this thread runs between two
+            // MMAs, so the ring position is carried incrementally (no division) and the stage
+            // descriptors advance by a fixed stride.
+            const uint64_t ad0 = sw128_kmajor_desc(sA), bd0 = sw128_kmajor_desc(sB);
+            constexpr uint64_t kAStep = PAIR_A_BYTES >> 4, kBStep = PAIR_B_BYTES >> 4;
+            int s = 0;
+            uint32_t ph = 0;
             int it = 0;
             for (int64_t t = cluster; t < pt.total && !*stop; t += nclusters, ++it) {
                 if (it > 0) {  // both epilogue groups have read the previous tile's accumulator
@@ -423,21 +437,22 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
                     }
                     tc_fence_after();
                 }
-                for (int kb = 0; kb < KB; ++kb, ++g) {
-                    const int s = (int)(g % PAIR_STAGES);
-                    const uint32_t ph = (uint32_t)((g / PAIR_STAGES) & 1);
+                for (int kb = 0; kb < KB; ++kb) {
                     const int w = mbar_wait_bounded(&full[s], ph, stop, err, abort, limit_ns);
                     if (w != kWaitOk) {
                         raise_stop(stop, err, w, site + kRoleMma * 10);
                         break;
                     }
                     tc_fence_after();
-                    const uint64_t ad = sw128_kmajor_desc(sA + s * PAIR_A_BYTES);
-                    const uint64_t bd = sw128_kmajor_desc(sB + s * PAIR_B_BYTES);
+                    const uint64_t ad = ad0 + (uint64_t)s * kAStep, bd = bd0 + (uint64_t)s * kBStep;
 #pragma unroll
                     for (int kk = 0; kk < MMAS_PER_STAGE; ++kk)
                         umma_pair<BF16>(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
                     umma_commit_pair(&empty[s]);
+                    if (++s == PAIR_STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
                 }
                 // The tile's accumulator is complete once the MMAs issued so far finish (on a
                 // stop: whatever was issued; the epilogue then skips the tile).
