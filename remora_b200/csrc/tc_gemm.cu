@@ -255,11 +255,12 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 // SM -- and then both wait forever.) A single-CTA tcgen05 kernel (at most 256 columns, it
 // waits on no other CTA) may run beside a pair CTA; the pair's collective allocation then
 // waits at most until that CTA finishes. Two configurations:
-//   PairCo    (3 stages, one 32-column box per warp, 113 KB): leaves room beside it for one
-//             single-CTA tcgen05 kernel (~97 KB) -- the factorisation's look-ahead chain
-//             runs there;
-//   PairAlone (5 stages, two 64-column boxes per warp, 225 KB): a deeper ring for a launch
-//             that runs alone (rc_syrk_tc).
+//   PairCo    (3 stages, one 32-column box per warp, 113 KB, one 256-column accumulator):
+//             leaves room beside it for one single-CTA tcgen05 kernel (~97 KB, at most 256
+//             TMEM columns) -- the factorisation's look-ahead chain runs there;
+//   PairAlone (5 stages, two 64-column boxes per warp, 225 KB, two 256-column accumulators:
+//             the MMAs of the next tile run while the epilogue drains the last one): a
+//             launch that has the SMs to itself (rc_syrk_tc, rc_gemm_tf32).
 //
 // Failure handling. Every mbarrier wait is bounded and gives up as soon as the device
 // error word or the abort word is raised; the epilogue warps take each decision together
@@ -269,9 +270,10 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 // resident for a settle period so that copies still in flight land first.
 constexpr int PAIR_A_BYTES = 128 * KB_BYTES, PAIR_B_BYTES = 128 * KB_BYTES;
 constexpr int PAIR_THREADS = 192;
-template <int STAGES_, int EPI_BLK_, int EPI_BUFS_>
+template <int STAGES_, int EPI_BLK_, int EPI_BUFS_, int TMEM_BUFS_>
 struct PairCfg {
     static constexpr int STAGES = STAGES_;
+    static constexpr int TMEM_BUFS = TMEM_BUFS_;               // 256-column accumulators per CTA
     static constexpr int EPI_BLK = EPI_BLK_;                   // 32-column blocks per staged box
     static constexpr int EPI_COLS = 32 * EPI_BLK;              // columns per box
     static constexpr int EPI_BOX_BYTES = 32 * EPI_COLS * 4;    // 32 rows
@@ -281,8 +283,8 @@ struct PairCfg {
 };
 // 115,968 bytes: with the 1 KB the hardware reserves per CTA, a 99,584-byte single-CTA
 // kernel still fits beside it in an SM's 233,472.
-using PairCo = PairCfg<3, 1, 1>;
-using PairAlone = PairCfg<5, 2, 2>;
+using PairCo = PairCfg<3, 1, 1, 1>;
+using PairAlone = PairCfg<5, 2, 2, 2>;
 static_assert(PairCo::SMEM + 1024 + 99584 + 1024 <= 233472, "a look-ahead CTA must fit beside a pair CTA");
 
 // The tile enumeration of one pair launch: mode 0 all tm_count x tn_count tiles, mode 1
@@ -351,14 +353,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;
     constexpr int PAIR_STAGES = Cfg::STAGES, EPI_COLS = Cfg::EPI_COLS, EPI_BOX_BYTES = Cfg::EPI_BOX_BYTES;
-    constexpr int EPI_BUFS = Cfg::EPI_BUFS;
+    constexpr int EPI_BUFS = Cfg::EPI_BUFS, TBUFS = Cfg::TMEM_BUFS;
+    constexpr uint32_t TMEM_COLS = 256u * TBUFS;
     uint8_t* sB = sA + PAIR_STAGES * PAIR_A_BYTES;
     uint8_t* stage_c = sB + PAIR_STAGES * PAIR_B_BYTES;  // 4 warps x EPI_BUFS boxes
     uint64_t* full = reinterpret_cast<uint64_t*>(stage_c + Cfg::STAGING);
     uint64_t* empty = full + PAIR_STAGES;
-    uint64_t* tfull = empty + PAIR_STAGES;
-    uint64_t* tempty = tfull + 1;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
+    uint64_t* tfull = empty + PAIR_STAGES;  // per accumulator buffer
+    uint64_t* tempty = tfull + TBUFS;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + TBUFS);
     volatile int* stop = reinterpret_cast<volatile int*>(tmem_slot + 1);
     volatile int* any_stop = stop + 1;
 
@@ -371,8 +374,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(tfull, 1);
-        mbar_init(tempty, 2);  // one arrival per CTA's epilogue group (used in the leader)
+        for (int b = 0; b < TBUFS; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 2);  // one arrival per CTA's epilogue group (used in the leader)
+        }
         // A word already raised stops this CTA's roles before they start (no early return:
         // the peer may have read the word as zero and waits at the cluster barriers).
         *stop = (aborted(abort) || aborted(err)) ? 1 : 0;
@@ -384,7 +389,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(256u));
+                     "r"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
     }
     tc_fence_before();
@@ -429,8 +434,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
             uint32_t ph = 0;
             int it = 0;
             for (int64_t t = cluster; t < pt.total && !*stop; t += nclusters, ++it) {
-                if (it > 0) {  // both epilogue groups have read the previous tile's accumulator
-                    const int w = mbar_wait_bounded(tempty, (uint32_t)((it - 1) & 1), stop, err, abort, limit_ns);
+                // Both epilogue groups have read the accumulator this tile reuses (tile
+                // it - TBUFS); a fresh barrier passes parity 1 at once.
+                const int ab = it % TBUFS;
+                const uint32_t acc_col = 256u * (uint32_t)ab;
+                {
+                    const int w = mbar_wait_bounded(&tempty[ab], (uint32_t)(((it / TBUFS) & 1) ^ 1), stop, err,
+                                                    abort, limit_ns);
                     if (w != kWaitOk) {
                         raise_stop(stop, err, w, site + kRoleMma * 10);
                         break;
@@ -447,7 +457,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
                     const uint64_t ad = ad0 + (uint64_t)s * kAStep, bd = bd0 + (uint64_t)s * kBStep;
 #pragma unroll
                     for (int kk = 0; kk < MMAS_PER_STAGE; ++kk)
-                        umma_pair<BF16>(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
+                        umma_pair<BF16>(tmem + acc_col, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0 ? 1u : 0u);
                     umma_commit_pair(&empty[s]);
                     if (++s == PAIR_STAGES) {
                         s = 0;
@@ -456,7 +466,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
                 }
                 // The tile's accumulator is complete once the MMAs issued so far finish (on a
                 // stop: whatever was issued; the epilogue then skips the tile).
-                umma_commit_pair(tfull);
+                umma_commit_pair(&tfull[ab]);
             }
         }
     } else {
@@ -466,7 +476,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
         const bool vec = C.cs == 1 && (C.rs % 4 == 0) && (reinterpret_cast<uintptr_t>(C.p) % 16 == 0);
         int it = 0, issued = 0;
         for (int64_t t = cluster; t < pt.total; t += nclusters, ++it) {
-            const int w = mbar_wait_bounded(tfull, (uint32_t)(it & 1), stop, err, abort, limit_ns);
+            const int ab = it % TBUFS;
+            const uint32_t tacc = tmem + 256u * (uint32_t)ab;
+            const int w = mbar_wait_bounded(&tfull[ab], (uint32_t)((it / TBUFS) & 1), stop, err, abort, limit_ns);
             // One decision for all epilogue warps (their barrier below counts them all).
             if (epilogue_any(w != kWaitOk || *stop, EPI_THREADS)) {
                 if (w != kWaitOk) raise_stop(stop, err, w, site + kRoleEpilogue * 10);
@@ -484,7 +496,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
 #pragma unroll 1
                 for (int c0 = 0; c0 < 256; c0 += EPI_COLS) {
                     float v[16];
-                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+                    tmem_ld16(tacc + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
                     uint8_t* box = my_stage + (issued % EPI_BUFS) * EPI_BOX_BYTES;
                     if (issued >= EPI_BUFS) {  // the box written EPI_BUFS steps ago has been read
                         if (lane == 0) bulk_wait_read<EPI_BUFS - 1>();
@@ -500,7 +512,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
                     }
 #pragma unroll
                     for (int sub = 16; sub < EPI_COLS; sub += 16) {
-                        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(c0 + sub), v);
+                        tmem_ld16(tacc + ((uint32_t)(32 * q) << 16) + (uint32_t)(c0 + sub), v);
                         uint8_t* blk = box + (sub / 32) * 4096;
 #pragma unroll
                         for (int u = 0; u < 4; ++u) {
@@ -523,7 +535,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
 #pragma unroll 1
                 for (int c0 = 0; c0 < 256; c0 += 16) {
                     float v[16];
-                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+                    tmem_ld16(tacc + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
                     if (!row_ok) continue;
                     const int64_t j0 = n0 + c0;
                     if (vec && j0 + 15 < N && keep(mask, 0, i, j0 + 15) && keep(mask, 0, i, j0)) {
@@ -554,7 +566,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
             // This CTA's reads of the accumulator are done: release it to the leader's MMAs.
             tc_fence_before();
             asm volatile("bar.sync 1, %0;" ::"r"(EPI_THREADS) : "memory");
-            if (warp == 2 && lane == 0) mbar_arrive_cluster(tempty, 0);
+            if (warp == 2 && lane == 0) mbar_arrive_cluster(&tempty[ab], 0);
         }
         if (lane == 0) bulk_wait_all();  // every reduce-add of this warp has landed
     }
@@ -568,7 +580,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
     cluster_sync_all();  // the leader's MMAs read this CTA's shared memory until its last tfull
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u));
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
     }
     if (threadIdx.x == 0 && *any_stop) settle(kSettleNs);
 }
