@@ -24,9 +24,10 @@
 // Per CTA: a 128-row x 64-column tile of C. Warp 0 streams, per 128-wide K block, the
 // seven 128-row slices of the A rows through a 7-deep ring and the seven 64-row slices of
 // the B rows (one 3-D TMA box) through a 2-deep ring; warp 1 issues the MMAs; warps 2..5
-// finish the tile: during the main loop they pull their rows of the C tile into L2, then
-// combine the accumulators into a staging tile in the (by then idle) A ring and update C a
-// row at a time across the lanes, so that every C access is coalesced. Every mbarrier wait
+// finish the tile: during the main loop they load their rows of the C tile into registers
+// (a row per load across the lanes), then combine the accumulators into a staging tile in the
+// (by then idle) A ring and update C a row at a time across the lanes, so that every C
+// access is coalesced and none waits after the MMAs. Every mbarrier wait
 // is bounded, as in the other tensor-core kernels.
 #include <climits>
 #include <cudaTypedefs.h>
@@ -105,13 +106,11 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, ui
         : "memory");
 }
 
-// 16 int32 accumulator columns of this warp's TMEM lanes, without waiting (tmem_wait_ld).
-__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
+// 8 int32 accumulator columns of this warp's TMEM lanes, without waiting (tmem_wait_ld).
+__device__ __forceinline__ void tmem_ld8_async(uint32_t taddr, uint32_t (&r)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
@@ -144,7 +143,8 @@ __device__ __forceinline__ double scale_pow2(double h, int e) {
 // The seven int32 accumulators v[0] (weight 1) .. v[6] (weight 2^-42) as one FP64 value:
 // v0 2^21 + v1 2^14 + v2 2^7 + v3 and v4 2^14 + v5 2^7 + v6 are exact in int64 (|v| < 2^31),
 // and exact in FP64 (below 2^53 and 2^46), so h has one rounding.
-__device__ __forceinline__ double combine7(const uint32_t (&v)[S][16], int x) {
+template <int W>
+__device__ __forceinline__ double combine7(const uint32_t (&v)[S][W], int x) {
     const long long hi = ((((long long)(int)v[0][x] * 128 + (int)v[1][x]) * 128 + (int)v[2][x]) * 128) + (int)v[3][x];
     const long long lo = ((long long)(int)v[4][x] * 128 + (int)v[5][x]) * 128 + (int)v[6][x];
     return fma((double)hi, 0x1p-21, (double)lo * 0x1p-42);
@@ -302,68 +302,59 @@ __global__ void __launch_bounds__(EMU_THREADS, 1)
         const int r0 = 32 * q;
         const int64_t i = i0 + r0 + lane;  // the row whose accumulators this thread reads
         const int ei = i < M ? rexp[a0 + i] : 0;
-        if (i < M && beta != 0.0) {  // while the main loop runs: this row of the C tile into L2
-            const double* crow = C + i * ldc + j0;
-            const int64_t cols = N - j0 < 64 ? N - j0 : 64;
-            for (int64_t c = 0; c < cols; c += 16) asm volatile("prefetch.global.L2 [%0];" ::"l"(crow + c));
-        }
+        // Tile-local indices: row rl = r0 + rr, column cl = lane + 32 u; C(rl, cl) is written
+        // when rl < mrem, cl < nrem and, for the lower triangle, cl - rl <= dlim.
+        const int mrem = (int)(M - i0 < 128 ? M - i0 : 128), nrem = (int)(N - j0 < 64 ? N - j0 : 64);
+        const int dlim = lower ? (int)(i0 - j0 < 256 ? i0 - j0 : 256) : 256;
+        const bool rd = beta != 0.0;
+        double* cw = C + (i0 + r0) * ldc + j0 + lane;  // this lane's column of the warp's first row
+        // While the main loop runs: the warp's 32 rows of the C tile (columns lane and
+        // lane + 32) into registers, a row per load across the lanes.
+        double cv[32][2];
+#pragma unroll
+        for (int rr = 0; rr < 32; ++rr)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int rl = r0 + rr, cl = lane + 32 * u;
+                cv[rr][u] = (rd && rl < mrem && cl < nrem && cl - rl <= dlim) ? cw[(int64_t)rr * ldc + 32 * u] : 0.0;
+            }
+        int ej[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) ej[u] = lane + 32 * u < nrem ? rexp[b0 + j0 + lane + 32 * u] : 0;
         const int w = mbar_wait_bounded(done, 0, stop, err, abort, limit_ns);
         const bool ok = w == kWaitOk;
         if (!ok) raise_stop(stop, err, w, kSiteEmu * 100 + kRoleEpilogue * 10);
         tc_fence_after();
         if (__all_sync(0xffffffffu, ok && !*stop)) {
-            // 1. The seven accumulators of this thread's row, combined into this warp's 32 rows of a staging tile in the operand ring, idle now that
-            //    every load has been consumed and every MMA has completed.
+            // 1. The seven accumulators of this thread's row, combined, into this warp's 32 rows
+            //    of a staging tile in the operand ring (idle now: every load has been consumed
+            //    and every MMA has completed).
             const uint32_t stage = smem_u32(sA) + (uint32_t)(r0 * kStageLd * 8);
             const uint32_t srow = stage + (uint32_t)(lane * kStageLd * 8);
 #pragma unroll 1
-            for (int cc = 0; cc < 64; cc += 16) {
-                uint32_t v[S][16];
+            for (int cc = 0; cc < 64; cc += 8) {
+                uint32_t v[S][8];
 #pragma unroll
-                for (int d = 0; d < S; ++d) tmem_ld16_async(tmem + ((uint32_t)r0 << 16) + (uint32_t)(64 * d + cc), v[d]);
+                for (int d = 0; d < S; ++d) tmem_ld8_async(tmem + ((uint32_t)r0 << 16) + (uint32_t)(64 * d + cc), v[d]);
                 tmem_wait_ld();
 #pragma unroll
-                for (int x = 0; x < 16; ++x) sts_f64(srow + (uint32_t)((cc + x) * 8), combine7(v, x));
+                for (int x = 0; x < 8; ++x) sts_f64(srow + (uint32_t)((cc + x) * 8), combine7(v, x));
             }
             __syncwarp();
-            // 2. The warp's 32 rows of C, a row at a time across the lanes (columns lane and
-            //    lane + 32): every C load of the 32 rows in flight at once, then the updates.
-            //    Tile-local indices: row rl = r0 + rr, column cl = lane + 32 u; C(rl, cl) is
-            //    written when rl < mrem, cl < nrem and, for the lower triangle, cl - rl <= dlim.
-            const int mrem = (int)(M - i0 < 128 ? M - i0 : 128), nrem = (int)(N - j0 < 64 ? N - j0 : 64);
-            const int dlim = lower ? (int)(i0 - j0 < 256 ? i0 - j0 : 256) : 256;
-            const bool rd = beta != 0.0;
-            int ej[2];
+            // 2. The warp's 32 rows of C, a row at a time across the lanes.
 #pragma unroll
-            for (int u = 0; u < 2; ++u) ej[u] = lane + 32 * u < nrem ? rexp[b0 + j0 + lane + 32 * u] : 0;
-            double* cw = C + (i0 + r0) * ldc + j0 + lane;  // this lane's column of the warp's first row
-#pragma unroll 1
-            for (int half = 0; half < 32; half += 16) {
-                double cv[16][2], hv[16][2];
+            for (int rr = 0; rr < 32; ++rr) {
+                const int rl = r0 + rr;
+                const int er = __shfl_sync(0xffffffffu, ei, rr);
 #pragma unroll
-                for (int rr = 0; rr < 16; ++rr) {
-                    const int rl = r0 + half + rr;
-#pragma unroll
-                    for (int u = 0; u < 2; ++u) {
-                        const int cl = lane + 32 * u;
-                        const bool live = rl < mrem && cl < nrem && cl - rl <= dlim;
-                        cv[rr][u] = (live && rd) ? cw[(int64_t)(half + rr) * ldc + 32 * u] : 0.0;
-                        hv[rr][u] = lds_f64(stage + (uint32_t)(((half + rr) * kStageLd + cl) * 8));
-                    }
-                }
-#pragma unroll
-                for (int rr = 0; rr < 16; ++rr) {
-                    const int rl = r0 + half + rr;
-                    const int er = __shfl_sync(0xffffffffu, ei, half + rr);
-#pragma unroll
-                    for (int u = 0; u < 2; ++u) {
-                        const int cl = lane + 32 * u;
-                        const bool bad = er == kOzBadExp || ej[u] == kOzBadExp;
-                        double val = scale_pow2(hv[rr][u], bad ? 0 : er + ej[u] - 14);
-                        val = bad ? __longlong_as_double(0x7FF8000000000000ll) : val;
-                        const double out = rd ? fma(alpha, val, beta * cv[rr][u]) : alpha * val;
-                        if (rl < mrem && cl < nrem && cl - rl <= dlim) cw[(int64_t)(half + rr) * ldc + 32 * u] = out;
-                    }
+                for (int u = 0; u < 2; ++u) {
+                    const int cl = lane + 32 * u;
+                    const double h = lds_f64(stage + (uint32_t)((rr * kStageLd + cl) * 8));
+                    const bool bad = er == kOzBadExp || ej[u] == kOzBadExp;
+                    double val = scale_pow2(h, bad ? 0 : er + ej[u] - 14);
+                    val = bad ? __longlong_as_double(0x7FF8000000000000ll) : val;
+                    const double out = rd ? fma(alpha, val, beta * cv[rr][u]) : alpha * val;
+                    if (rl < mrem && cl < nrem && cl - rl <= dlim) cw[(int64_t)rr * ldc + 32 * u] = out;
                 }
             }
         }
