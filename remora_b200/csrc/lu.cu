@@ -116,6 +116,197 @@ __global__ void __launch_bounds__(kLuThreads) getrf_panel_kernel(int64_t n, View
     }
 }
 
+// The same panel factorisation spread over a cooperative grid: CTA b holds rows
+// [k0 + b chunk, k0 + (b + 1) chunk) of the panel in shared memory (row stride nb + 1), and
+// one bounded grid barrier per column exchanges what the next column needs. For column j
+// (c = k0 + j), after the barrier every CTA reduces the published candidates in the same
+// order (so all agree on the pivot p) and reads p's row; the owners of rows c and p swap
+// them; then, with a look-ahead of one column:
+//   1. every row below c is divided by the pivot and only its column j + 1 is updated;
+//   2. the CTA's candidate for column j + 1 (largest |A(i, c + 1)|, i > c, the lowest row
+//      among equals) and row c + 1 are updated in full and published;
+//   3. the CTA arrives at the barrier, applies the rest of the rank-1 update to its other
+//      rows while the others arrive, and waits.
+// Each element sees exactly the operations of getrf_panel_kernel, in the same order.
+constexpr int kCoopThreads = 256;
+constexpr int kCoopMaxChunk = 384;  // rows per CTA (shared memory: 384 x 65 doubles)
+
+struct CoopScratch {  // indexed by column j; the barrier words live separately
+    double* cand_v;   // [nb][G]
+    int64_t* cand_i;  // [nb][G]
+    double* cand_row; // [nb][G][nb]
+    double* crow;     // [nb][nb]: row c before the swap
+};
+
+// Grid barrier over nblocks co-resident CTAs (a cooperative launch), split into an arrival
+// and a wait so that work can run in between: bar[0] counts arrivals, bar[1] is the
+// generation. The wait is bounded by the SM's cycle counter (2 cycles per ns of the
+// library's wait limit); a timeout records RC_ERR_TIMEOUT in the error word and the caller
+// leaves.
+__device__ void grid_arrive(unsigned* bar, unsigned nblocks, unsigned gen) {
+    __syncthreads();  // every thread's stores before the arrival
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&bar[0], 1u) == nblocks - 1) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicExch(&bar[1], gen + 1u);
+        }
+    }
+}
+__device__ bool grid_wait(unsigned* bar, unsigned& gen, uint64_t limit_ns, int* err, int* pass) {
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const long long t0 = clock64(), lim = (long long)(limit_ns * 2u);
+        while (*(volatile unsigned*)&bar[1] == gen) {
+            if (clock64() - t0 > lim) {
+                ok = 0;
+                if (err && atomicCAS(err, 0, RC_ERR_TIMEOUT) == 0) atomicExch(err + 1, 500);
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+        *pass = ok;
+    }
+    __syncthreads();
+    ++gen;
+    return *pass != 0;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kCoopThreads, 1)
+    getrf_panel_coop_kernel(int64_t n, View<T> A, int64_t k0, int nb, int chunk, int* piv, int* info,
+                            CoopScratch sc, unsigned* bar, int* err, uint64_t limit_ns) {
+    extern __shared__ unsigned char coop_smem[];
+    T* P = reinterpret_cast<T*>(coop_smem);  // chunk x (nb + 1)
+    double* prow = reinterpret_cast<double*>(coop_smem) + ((size_t)chunk * (nb + 1) * sizeof(T) + 7) / 8;  // nb
+    double* sv = prow + kLuNB;                                // 32
+    int64_t* si = reinterpret_cast<int64_t*>(sv + 32);        // 32
+    int* pass = reinterpret_cast<int*>(si + 32);
+    const int ld = nb + 1, G = (int)gridDim.x, b = (int)blockIdx.x;
+    if (*(volatile int*)info != 0) return;
+    const int64_t base = k0 + (int64_t)b * chunk;
+    const int myrows = (int)(n - base < chunk ? (n - base > 0 ? n - base : 0) : chunk);
+    for (int e = threadIdx.x; e < myrows * nb; e += kCoopThreads) {
+        const int r = e / nb, col = e % nb;
+        P[r * ld + col] = A(base + r, k0 + col);
+    }
+    __syncthreads();
+    // Publish the candidate for column j (rows >= k0 + j) and row k0 + j; both fully updated.
+    auto publish = [&](int j, double best, int64_t bi) {
+        const int64_t c = k0 + j;
+        if (threadIdx.x == 0) {
+            sc.cand_v[(size_t)j * G + b] = best;
+            sc.cand_i[(size_t)j * G + b] = bi;
+        }
+        if (bi != INT64_MAX) {
+            double* dst = sc.cand_row + ((size_t)j * G + b) * nb;
+            for (int col = threadIdx.x; col < nb; col += kCoopThreads) dst[col] = (double)P[(bi - base) * ld + col];
+        }
+        if (c >= base && c < base + myrows)
+            for (int col = threadIdx.x; col < nb; col += kCoopThreads)
+                sc.crow[(size_t)j * nb + col] = (double)P[(c - base) * ld + col];
+    };
+    auto local_argmax = [&](int j, double& best, int64_t& bi) {
+        const int64_t c = k0 + j;
+        best = -1.0;
+        bi = INT64_MAX;
+        for (int r = threadIdx.x; r < myrows; r += kCoopThreads) {
+            const int64_t i = base + r;
+            if (i < c) continue;
+            const double a = fabs((double)P[r * ld + j]);
+            if (a > best || (a == best && i < bi)) {
+                best = a;
+                bi = i;
+            }
+        }
+        block_argmax(best, bi, sv, si);
+    };
+    unsigned gen = 0;
+    {  // column 0 needs no update first
+        double best;
+        int64_t bi;
+        local_argmax(0, best, bi);
+        publish(0, best, bi);
+        grid_arrive(bar, (unsigned)G, gen);
+        if (!grid_wait(bar, gen, limit_ns, err, pass)) return;
+    }
+    for (int j = 0; j < nb; ++j) {
+        const int64_t c = k0 + j;
+        // The pivot: every CTA reduces the G candidates in the same order.
+        double best = -1.0;
+        int64_t bi = INT64_MAX;
+        for (int q = threadIdx.x; q < G; q += kCoopThreads) {
+            const double v = __ldcg(sc.cand_v + (size_t)j * G + q);
+            const int64_t i = __ldcg(sc.cand_i + (size_t)j * G + q);
+            if (v > best || (v == best && i < bi)) {
+                best = v;
+                bi = i;
+            }
+        }
+        block_argmax(best, bi, sv, si);
+        const int64_t p = bi;
+        const int owner = (int)((p - k0) / chunk);
+        const double* pr = sc.cand_row + ((size_t)j * G + owner) * nb;
+        for (int col = threadIdx.x; col < nb; col += kCoopThreads) prow[col] = __ldcg(pr + col);
+        __syncthreads();
+        const double pv = prow[j];
+        if (pv == 0.0) {  // also all-zero columns: the first row is the pivot, value 0
+            if (b == 0 && threadIdx.x == 0) {
+                piv[c] = (int)c;
+                record_first(info, (int)(c + 1));
+            }
+            return;
+        }
+        if (b == 0 && threadIdx.x == 0) piv[c] = (int)p;
+        if (p != c) {
+            if (c >= base && c < base + myrows)
+                for (int col = threadIdx.x; col < nb; col += kCoopThreads) P[(c - base) * ld + col] = (T)prow[col];
+            if (p >= base && p < base + myrows)
+                for (int col = threadIdx.x; col < nb; col += kCoopThreads)
+                    P[(p - base) * ld + col] = (T)__ldcg(sc.crow + (size_t)j * nb + col);
+        }
+        __syncthreads();
+        // 1. divide, and update column j + 1 only
+        for (int r = threadIdx.x; r < myrows; r += kCoopThreads) {
+            if (base + r <= c) continue;
+            T* row = P + r * ld;
+            const T l = (T)((double)row[j] / pv);
+            row[j] = l;
+            if (j + 1 < nb) row[j + 1] -= l * (T)prow[j + 1];
+        }
+        __syncthreads();
+        if (j + 1 == nb) break;
+        // 2. the candidate for column j + 1 and row c + 1, updated in full and published
+        local_argmax(j + 1, best, bi);
+        const int64_t rc1 = c + 1;
+        const bool own_c1 = rc1 >= base && rc1 < base + myrows;
+        const int ra = bi != INT64_MAX ? (int)(bi - base) : -1;
+        const int rb = own_c1 ? (int)(rc1 - base) : -1;
+        for (int col = j + 2 + threadIdx.x; col < nb; col += kCoopThreads) {
+            if (ra >= 0) P[ra * ld + col] -= P[ra * ld + j] * (T)prow[col];
+            if (rb >= 0 && rb != ra) P[rb * ld + col] -= P[rb * ld + j] * (T)prow[col];
+        }
+        __syncthreads();
+        publish(j + 1, best, bi);
+        grid_arrive(bar, (unsigned)G, gen);
+        // 3. the rest of the rank-1 update while the other CTAs arrive
+        for (int r = threadIdx.x; r < myrows; r += kCoopThreads) {
+            if (base + r <= c || r == ra || r == rb) continue;
+            T* row = P + r * ld;
+            const T l = row[j];
+            for (int col = j + 2; col < nb; ++col) row[col] -= l * (T)prow[col];
+        }
+        if (!grid_wait(bar, gen, limit_ns, err, pass)) return;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < myrows * nb; e += kCoopThreads) {
+        const int r = e / nb, col = e % nb;
+        A(base + r, k0 + col) = P[r * ld + col];
+    }
+}
+
 // The row swaps piv[k0 .. k0 + nb) in order, on the columns outside the panel.
 template <class T>
 __global__ void lu_swap_kernel(int64_t n, View<T> A, int64_t k0, int nb, const int* piv, const int* info) {
@@ -226,14 +417,57 @@ View<T> view_of(int row_major, T* A, int64_t lda) {
     return row_major ? View<T>{A, lda, 1} : View<T>{A, 1, lda};
 }
 
+// The panel on a cooperative grid of about 256 rows per CTA (a grid barrier costs more the
+// more CTAs meet at it, the column work per CTA grows with its rows), at most one CTA per
+// SM; on one CTA when the panel's rows do not fit the grid's shared memory (n above ~56K).
+constexpr int kCoopRows = 256;
+template <class T>
+int getrf_panel(int64_t n, View<T> A, int64_t k0, int nb, int* piv, int* info, cudaStream_t s) {
+    const int64_t rows = n - k0;
+    const int sms = sm_count();
+    int G = (int)((rows + kCoopRows - 1) / kCoopRows);
+    if (G > sms) G = sms;
+    const int chunk = (int)((rows + G - 1) / G);
+    if (chunk > kCoopMaxChunk || sms <= 0) {
+        getrf_panel_kernel<T><<<1, kLuThreads, 0, s>>>(n, A, k0, nb, piv, info);
+        return check_launch();
+    }
+    const size_t panel_bytes = ((size_t)chunk * (nb + 1) * sizeof(T) + 7) / 8 * 8;
+    const size_t smem = panel_bytes + (kLuNB + 32) * sizeof(double) + 32 * sizeof(int64_t) + 16;
+    const size_t n_cand = (size_t)kLuNB * sms;
+    const size_t bytes = 256 + n_cand * (sizeof(double) + sizeof(int64_t)) + n_cand * kLuNB * sizeof(double) +
+                         (size_t)kLuNB * kLuNB * sizeof(double);
+    char* ws = static_cast<char*>(workspace(s, bytes, 14));
+    if (!ws) return RC_ERR_ALLOC;
+    unsigned* bar = reinterpret_cast<unsigned*>(ws);
+    CoopScratch sc;
+    sc.cand_v = reinterpret_cast<double*>(ws + 256);
+    sc.cand_i = reinterpret_cast<int64_t*>(sc.cand_v + n_cand);
+    sc.cand_row = reinterpret_cast<double*>(sc.cand_i + n_cand);
+    sc.crow = sc.cand_row + n_cand * kLuNB;
+    if (cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s) != cudaSuccess) return RC_ERR_CUDA;
+    if (cudaFuncSetAttribute(getrf_panel_coop_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return RC_ERR_CUDA;
+    int* err = error_word();
+    uint64_t lim = wait_limit_ns();
+    void* args[] = {&n, &A, &k0, &nb, const_cast<int*>(&chunk), &piv, &info, &sc, &bar, &err, &lim};
+    if (cudaLaunchCooperativeKernel((const void*)getrf_panel_coop_kernel<T>, dim3((unsigned)G), dim3(kCoopThreads),
+                                    args, smem, s) != cudaSuccess) {
+        cudaGetLastError();
+        return RC_ERR_CUDA;
+    }
+    count_launch();
+    return RC_SUCCESS;
+}
+
 template <class T>
 int getrf(int row_major, int64_t n, T* Ap, int64_t lda, int* piv, int* info, cudaStream_t s) {
     if (cudaMemsetAsync(info, 0, sizeof(int), s) != cudaSuccess) return RC_ERR_CUDA;
     const View<T> A = view_of(row_major, Ap, lda);
     for (int64_t k0 = 0; k0 < n; k0 += kLuNB) {
         const int nb = (int)(n - k0 < kLuNB ? n - k0 : kLuNB);
-        getrf_panel_kernel<T><<<1, kLuThreads, 0, s>>>(n, A, k0, nb, piv, info);
-        RC_TRY(check_launch());
+        RC_TRY(getrf_panel<T>(n, A, k0, nb, piv, info, s));
         if (n > nb) {
             const int64_t cols = n - nb;
             lu_swap_kernel<T><<<ceil_div(cols, 256) < 1024u ? ceil_div(cols, 256) : 1024u, 256, 0, s>>>(n, A, k0, nb,

@@ -65,6 +65,43 @@ def test_getrf_random(cuda, orc, n):
     _lu_check(A, to_host(Ad), piv2, 1e-13)
 
 
+def test_getrf_multi_cta_panel_2048(cuda, orc):
+    """n = 2048: the panels run on a cooperative grid (up to one CTA per SM, one grid
+    barrier per column); the pivots are the oracle's and P L U = A within 1e-13."""
+    n = 2048
+    rs = np.random.default_rng(2048)
+    A = rs.uniform(-1, 1, (n, n))
+    Ad = to_dev(A, True)
+    info, piv = ops.getrf(Ad)
+    assert info == 0
+    F2 = np.array(A, order="F")
+    st, piv2 = orc.getrf(F2)
+    assert st == 0 and np.array_equal(piv.cpu().numpy(), piv2)
+    _lu_check(A, to_host(Ad), piv2, 1e-13)
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-13), (torch.float32, 1e-4)])
+def test_getrf_8192_residual(cuda, dtype, tol):
+    """n = 8192 on the device: P L U = A (relative Frobenius) with the returned pivots."""
+    n = 8192
+    g = torch.Generator(device="cuda").manual_seed(81)
+    A = torch.rand((n, n), generator=g, device="cuda", dtype=dtype) * 2 - 1
+    F = A.clone()
+    info, piv = ops.getrf(F)
+    assert info == 0
+    L = torch.tril(F.double(), -1) + torch.eye(n, device="cuda", dtype=torch.float64)
+    U = torch.triu(F.double())
+    PA = A.double().clone()
+    p = piv.cpu().numpy()
+    perm = np.arange(n)
+    for i, q in enumerate(p):
+        if q != i:
+            perm[[i, q]] = perm[[q, i]]
+    PA = PA[torch.from_numpy(perm).cuda()]
+    rel = float(torch.linalg.norm(L @ U - PA) / torch.linalg.norm(PA))
+    assert rel <= tol
+
+
 def test_getrf_f32(cuda, golden):
     g = golden("lu_pstrf")
     A = g["lu123_A"]
