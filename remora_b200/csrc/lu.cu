@@ -177,7 +177,7 @@ __device__ bool grid_wait(unsigned* bar, unsigned& gen, uint64_t limit_ns, int* 
 template <class T>
 __global__ void __launch_bounds__(kCoopThreads, 1)
     getrf_panel_coop_kernel(int64_t n, View<T> A, int64_t k0, int nb, int chunk, int* piv, int* info,
-                            CoopScratch sc, unsigned* bar, int* err, uint64_t limit_ns) {
+                            CoopScratch sc, unsigned* bar, int* err, uint64_t limit_ns, T* linv) {
     extern __shared__ unsigned char coop_smem[];
     T* P = reinterpret_cast<T*>(coop_smem);  // chunk x (nb + 1)
     double* prow = reinterpret_cast<double*>(coop_smem) + ((size_t)chunk * (nb + 1) * sizeof(T) + 7) / 8;  // nb
@@ -305,6 +305,27 @@ __global__ void __launch_bounds__(kCoopThreads, 1)
         const int r = e / nb, col = e % nb;
         A(base + r, k0 + col) = P[r * ld + col];
     }
+    if (b != 0) return;
+    // CTA 0 holds L11 (rows k0 .. k0 + nb, unit lower): its inverse, in place over L11 in
+    // shared memory, column by column from the last (X L = I gives, for q > j,
+    // X(q, j) = -(L(q, j) + sum_{j < m < q} X(q, m) L(m, j)), columns m > j already final),
+    // then to linv (row-major nb x nb) for the TRSM of the rows right of the panel.
+    __syncthreads();
+    for (int j = nb - 2; j >= 0; --j) {
+        const int q = j + 1 + threadIdx.x;
+        T v = 0;
+        if (q < nb) {
+            v = P[q * ld + j];
+            for (int m = j + 1; m < q; ++m) v += P[q * ld + m] * P[m * ld + j];
+        }
+        __syncthreads();
+        if (q < nb) P[q * ld + j] = -v;
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < nb * nb; e += kCoopThreads) {
+        const int q = e / nb, m = e % nb;
+        linv[e] = q > m ? P[q * ld + m] : (q == m ? T(1) : T(0));
+    }
 }
 
 // The row swaps piv[k0 .. k0 + nb) in order, on the columns outside the panel.
@@ -421,8 +442,11 @@ View<T> view_of(int row_major, T* A, int64_t lda) {
 // more CTAs meet at it, the column work per CTA grows with its rows), at most one CTA per
 // SM; on one CTA when the panel's rows do not fit the grid's shared memory (n above ~56K).
 constexpr int kCoopRows = 256;
+// linv (device, nb x nb): receives inv(L11) when the cooperative form ran (*have_inv).
 template <class T>
-int getrf_panel(int64_t n, View<T> A, int64_t k0, int nb, int* piv, int* info, cudaStream_t s) {
+int getrf_panel(int64_t n, View<T> A, int64_t k0, int nb, int* piv, int* info, T* linv, bool* have_inv,
+                cudaStream_t s) {
+    *have_inv = false;
     const int64_t rows = n - k0;
     const int sms = sm_count();
     int G = (int)((rows + kCoopRows - 1) / kCoopRows);
@@ -451,13 +475,14 @@ int getrf_panel(int64_t n, View<T> A, int64_t k0, int nb, int* piv, int* info, c
         return RC_ERR_CUDA;
     int* err = error_word();
     uint64_t lim = wait_limit_ns();
-    void* args[] = {&n, &A, &k0, &nb, const_cast<int*>(&chunk), &piv, &info, &sc, &bar, &err, &lim};
+    void* args[] = {&n, &A, &k0, &nb, const_cast<int*>(&chunk), &piv, &info, &sc, &bar, &err, &lim, &linv};
     if (cudaLaunchCooperativeKernel((const void*)getrf_panel_coop_kernel<T>, dim3((unsigned)G), dim3(kCoopThreads),
                                     args, smem, s) != cudaSuccess) {
         cudaGetLastError();
         return RC_ERR_CUDA;
     }
     count_launch();
+    *have_inv = true;
     return RC_SUCCESS;
 }
 
@@ -465,9 +490,12 @@ template <class T>
 int getrf(int row_major, int64_t n, T* Ap, int64_t lda, int* piv, int* info, cudaStream_t s) {
     if (cudaMemsetAsync(info, 0, sizeof(int), s) != cudaSuccess) return RC_ERR_CUDA;
     const View<T> A = view_of(row_major, Ap, lda);
+    T* linv = static_cast<T*>(workspace(s, (size_t)kLuNB * kLuNB * sizeof(T), 16));
+    if (!linv) return RC_ERR_ALLOC;
     for (int64_t k0 = 0; k0 < n; k0 += kLuNB) {
         const int nb = (int)(n - k0 < kLuNB ? n - k0 : kLuNB);
-        RC_TRY(getrf_panel<T>(n, A, k0, nb, piv, info, s));
+        bool have_inv = false;
+        RC_TRY(getrf_panel<T>(n, A, k0, nb, piv, info, linv, &have_inv, s));
         if (n > nb) {
             const int64_t cols = n - nb;
             lu_swap_kernel<T><<<ceil_div(cols, 256) < 1024u ? ceil_div(cols, 256) : 1024u, 256, 0, s>>>(n, A, k0, nb,
@@ -476,8 +504,14 @@ int getrf(int row_major, int64_t n, T* Ap, int64_t lda, int* piv, int* info, cud
         }
         const int64_t r = n - k0 - nb;
         if (r <= 0) continue;
-        const View<const T> L11{A.sub(k0, k0).p, A.rs, A.cs};
-        RC_TRY(trsm_left<T>(false, true, nb, r, T(1), L11, A.sub(k0, k0 + nb), nullptr, s, info));
+        if (have_inv) {  // U12 = inv(L11) A12, in place (the GEMM's single row tile reads all of A12's k range first)
+            const View<T> A12 = A.sub(k0, k0 + nb);
+            RC_TRY(gemm<T>(nb, r, nb, T(1), View<const T>{linv, kLuNB, 1}, View<const T>{A12.p, A12.rs, A12.cs},
+                           T(0), A12, kFull, 0, s, info));
+        } else {
+            const View<const T> L11{A.sub(k0, k0).p, A.rs, A.cs};
+            RC_TRY(trsm_left<T>(false, true, nb, r, T(1), L11, A.sub(k0, k0 + nb), nullptr, s, info));
+        }
         const View<const T> L21{A.sub(k0 + nb, k0).p, A.rs, A.cs}, U12{A.sub(k0, k0 + nb).p, A.rs, A.cs};
         RC_TRY(gemm<T>(r, r, nb, T(-1), L21, U12, T(1), A.sub(k0 + nb, k0 + nb), kFull, 0, s, info));
     }
