@@ -212,9 +212,25 @@ __global__ void __launch_bounds__(256, 1) potrf_diag(View<T> A, int sz, int64_t 
     if (aborted(info)) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool rowmaj = A.cs == 1;
-    for (int e = tid; e < NB * NB; e += 256) {
-        const int i = rowmaj ? e / NB : e % NB, c = rowmaj ? e % NB : e / NB;
-        S[i * SLD + c] = (i < sz && c < sz && c <= i) ? (double)A(i, c) : (i == c ? 1.0 : 0.0);
+    // The block into shared memory, 16 loads per thread in flight at a time (the block was
+    // just written by the previous update and comes from L2: one round trip per batch).
+    constexpr int kPer = NB * NB / 256, kBatch = 16;
+    static_assert(kPer % kBatch == 0, "load batches");
+#pragma unroll 1
+    for (int b0 = 0; b0 < kPer; b0 += kBatch) {
+        double v[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int e = tid + 256 * (b0 + u);
+            const int i = rowmaj ? e / NB : e % NB, c = rowmaj ? e % NB : e / NB;
+            v[u] = (i < sz && c < sz && c <= i) ? (double)A(i, c) : (i == c ? 1.0 : 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int e = tid + 256 * (b0 + u);
+            const int i = rowmaj ? e / NB : e % NB, c = rowmaj ? e % NB : e / NB;
+            S[i * SLD + c] = v[u];
+        }
     }
     if (tid == 0) *fail = 0;
     __syncthreads();
