@@ -278,40 +278,58 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            int a_used = 0;
-            for (int kb = 0; kb < KB && !*stop; ++kb) {
+            // The tensor pipe idles through every instruction this thread runs between two
+            // MMAs: the slices are unrolled with their shapes precomputed, and the A stage
+            // and its phase are carried incrementally.
+            uint32_t id1[S], id2[S];
+#pragma unroll
+            for (int t = 0; t < S; ++t) {
+                const int n_all = nr * (S - t);
+                id1[t] = i8_idesc(n_all < 256 ? n_all : 256);
+                id2[t] = i8_idesc(n_all > 256 ? n_all - 256 : 16);
+            }
+            const uint64_t ad0 = sw128_kmajor_desc(sA);
+            constexpr uint64_t kAStep = A_TILE >> 4;
+            const uint64_t b0d0 = sw128_kmajor_desc(sB), b0d1 = sw128_kmajor_desc(sB + 256 * 128);
+            const uint64_t b1d0 = sw128_kmajor_desc(sB + b_bytes), b1d1 = sw128_kmajor_desc(sB + b_bytes + 256 * 128);
+            int as = 0;
+            uint32_t aph = 0;
+            bool ok = true;
+            for (int kb = 0; kb < KB && ok; ++kb) {
                 const int bs = kb & 1;
-                const int w = mbar_wait_bounded(&bfull[bs], (kb >> 1) & 1, stop, err, nullptr, limit_ns);
+                int w = mbar_wait_bounded(&bfull[bs], (kb >> 1) & 1, stop, err, nullptr, limit_ns);
                 if (w != kWaitOk) {
                     raise_stop(stop, err, w, kSiteOzaki * 100 + kRoleMma * 10);
                     break;
                 }
                 tc_fence_after();
-                const uint64_t bd0 = sw128_kmajor_desc(sB + bs * b_bytes);
-                const uint64_t bd1 = sw128_kmajor_desc(sB + bs * b_bytes + 256 * 128);
+                const uint64_t bd0 = bs ? b1d0 : b0d0, bd1 = bs ? b1d1 : b0d1;
+#pragma unroll
                 for (int t = 0; t < S; ++t) {
-                    const int as = a_used % A_STAGES;
-                    const int wa = mbar_wait_bounded(&afull[as], (a_used / A_STAGES) & 1, stop, err, nullptr, limit_ns);
-                    if (wa != kWaitOk) {
-                        raise_stop(stop, err, wa, kSiteOzaki * 100 + kRoleMma * 10);
+                    w = mbar_wait_bounded(&afull[as], aph, stop, err, nullptr, limit_ns);
+                    if (w != kWaitOk) {
+                        raise_stop(stop, err, w, kSiteOzaki * 100 + kRoleMma * 10);
+                        ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint64_t ad = sw128_kmajor_desc(sA + as * A_TILE);
+                    const uint64_t ad = ad0 + (uint64_t)as * kAStep;
                     // A_t x [P_1 .. P_(S-t)] -> accumulators d = t+2 .. S+1 (columns nr t ..)
-                    const int n_all = nr * (S - t);
-                    const int n1 = n_all < 256 ? n_all : 256;
+                    const bool two = nr * (S - t) > 256;
                     const uint32_t col = (uint32_t)(nr * t);
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk) {
                         const uint32_t acc = (kb | t | kk) != 0 ? 1u : 0u;
-                        umma_i8(tmem + col, ad + 2 * kk, bd0 + 2 * kk, i8_idesc(n1), acc);
-                        if (n_all > 256) umma_i8(tmem + col + 256, ad + 2 * kk, bd1 + 2 * kk, i8_idesc(n_all - 256), acc);
+                        umma_i8(tmem + col, ad + 2 * kk, bd0 + 2 * kk, id1[t], acc);
+                        if (two) umma_i8(tmem + col + 256, ad + 2 * kk, bd1 + 2 * kk, id2[t], acc);
                     }
                     umma_commit(&aempty[as]);
-                    ++a_used;
+                    if (++as == A_STAGES) {
+                        as = 0;
+                        aph ^= 1u;
+                    }
                 }
-                umma_commit(&bempty[bs]);
+                if (ok) umma_commit(&bempty[bs]);
             }
             umma_commit(done);
         }
