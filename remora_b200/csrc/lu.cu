@@ -421,9 +421,21 @@ __global__ void __launch_bounds__(kLuThreads) pstrf_block_kernel(int64_t n, View
             return;
         }
         const T d = sqrt(v);
+        // Row c's block columns in shared memory; each row's block entries loaded 8 at a time
+        // (independent loads in flight), the dot product accumulated in the same order.
+        __shared__ T rowc[kPsNB];
+        if (threadIdx.x < j) rowc[threadIdx.x] = A(c, k + threadIdx.x);
+        __syncthreads();
         for (int64_t i = c + 1 + threadIdx.x; i < n; i += blockDim.x) {
             T s = A(i, c);
-            for (int64_t t = k; t < c; ++t) s -= A(i, t) * A(c, t);
+            for (int t0 = 0; t0 < j; t0 += 8) {
+                T a[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) a[u] = t0 + u < j ? A(i, k + t0 + u) : T(0);
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (t0 + u < j) s -= a[u] * rowc[t0 + u];
+            }
             A(i, c) = s / d;
         }
         __syncthreads();
