@@ -169,7 +169,14 @@ __global__ void __launch_bounds__(256, 1) gemm_dmma_f64(int64_t m, int64_t n, in
     extern __shared__ __align__(16) double dsmem[];
     double* sA = dsmem;
     double* sB = dsmem + DSTAGES * DK * DLDA;
-    const int64_t m0 = (int64_t)blockIdx.y * DM, n0 = (int64_t)blockIdx.x * BN;
+    // Grouped tile order: consecutive CTAs take kGroupM row tiles of one column tile before
+    // the next column tile, so that a wave holds a few A row blocks and B column blocks in L2
+    // instead of streaming all of B once per row of tiles.
+    constexpr int64_t kGroupM = 8;
+    const int64_t lin = (int64_t)blockIdx.y * gridDim.x + blockIdx.x, per = kGroupM * gridDim.x;
+    const int64_t first = lin / per * kGroupM, rest = (int64_t)gridDim.y - first;
+    const int64_t gsz = rest < kGroupM ? rest : kGroupM, r = lin % per;
+    const int64_t m0 = (first + r % gsz) * DM, n0 = r / gsz * BN;
     if (aborted(abort) || tile_outside(mask, off, m0, n0, DM, BN)) return;
     if (gridDim.z > 1) {  // K slice of a split-K product
         const int64_t kz = (int64_t)blockIdx.z * kchunk;
