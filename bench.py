@@ -474,7 +474,8 @@ def run_ours(args) -> None:
             "value": world * args.steps * flops(n, nrhs) / t / 1e12,
             "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 (factor: fp32 storage, " + args.precision + " tensor products)",
+            "vs_baseline": None, "dtype": ("f64 (factor: fp64 storage, int8 digit-product trailing updates)" if args.precision == "emu64"
+                      else "f64 (factor: fp32 storage, " + args.precision + " tensor products)"),
             "data": "synthetic (seeded Q diag(lambda) Q^T, N(0,1) right-hand sides)",
             "config": workload_config(args, world),
             "mixed": {"converged": status_ok, "backward_error": mixed_bwd, "cg_iterations": last["iterations"],
