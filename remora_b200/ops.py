@@ -109,6 +109,18 @@ def syrk(A: torch.Tensor, C: torch.Tensor, alpha: float = 1.0, upper: bool = Fal
     call(f"rc_syrk_{sfx}", int(up), ta, n, k, alpha, _ptr(A), lda, beta, _ptr(C), ldc, _stream())
 
 
+def syrk_emu64(P: torch.Tensor, C: torch.Tensor, alpha: float = 1.0, beta: float = 1.0) -> None:
+    """Lower triangle of C <- alpha * P @ P^T + beta * C in emulated FP64 (7 int8 digits per
+    entry of P, exact digit-pair products on the tensor cores): P and C row-major FP64 with
+    any row strides. The strict upper triangle of C is untouched."""
+    if P.dtype != torch.float64 or C.dtype != torch.float64:
+        raise TypeError("syrk_emu64 takes FP64 matrices")
+    n, k = P.shape
+    if C.shape != (n, n) or P.stride(1) != 1 or C.stride(1) != 1:
+        raise ValueError("syrk_emu64: P (n x k) and C (n x n) must be row-major")
+    call("rc_syrk_emu64", n, k, alpha, _ptr(P), P.stride(0), beta, _ptr(C), C.stride(0), _stream())
+
+
 def trsm(A: torch.Tensor, B: torch.Tensor, upper: bool = False, unit: bool = False, left: bool = True,
          alpha: float = 1.0, info: torch.Tensor | None = None) -> None:
     """B <- alpha * A^-1 B (left) or alpha * B A^-1 (right), A the named triangle."""
