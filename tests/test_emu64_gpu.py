@@ -150,3 +150,24 @@ def test_mixed_solve_emu64_not_spd_reports_pivot(cuda):
     A[200, 200] = -1.0
     X, info, status = ops.spd_solve_mixed(to_dev(A, False), to_dev(np.ones((n, 2)), False), "emu64", outer=128)
     assert info["pivot"] == 201
+
+
+def test_syrk_emu64_matches_the_restatement(cuda):
+    """General FP64 rows against the CPU restatement of the same digit-product method
+    (oracle/emu64.py: the same digits, the same 28 pairs, the same single rounding of their
+    combination), which leaves the truncation out of the comparison: the two agree to the
+    rounding of the combination (16 2^-53 (|P| |P|^T)), hundreds of times tighter than the
+    truncation bound, so a slice, pair, weight or sign out of place cannot pass."""
+    from oracle import emu64
+    rs = np.random.default_rng(77)
+    n, k = 200, 300
+    Ph = rs.standard_normal((n, k)) * np.exp2(rs.integers(-20, 21, size=(n, 1)))
+    ref = emu64.syrk_emu64(Ph)
+    P = torch.from_numpy(Ph).cuda()
+    C = torch.full((n, n), float("nan"), device="cuda", dtype=torch.float64)
+    assert _syrk_emu(P, C, 1.0, 0.0) == 0
+    Ch = to_host(C)
+    low = np.tril(np.ones((n, n), dtype=bool))
+    bound = 16 * U64 * (np.abs(Ph) @ np.abs(Ph).T)
+    assert np.all(np.abs(Ch - ref)[low] <= bound[low])
+    assert np.all(np.isnan(Ch[~low]))
