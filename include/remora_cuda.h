@@ -47,11 +47,11 @@ unsigned long long rc_allocation_count(void);
 /* Free every cached workspace of the current device (synchronises the device). */
 int rc_release_workspaces(void);
 /* Failure detection. Every device-side wait (the mbarrier phases of the tensor-core
- * pipelines) is bounded: by the SM's cycle counter, 2 cycles per nanosecond of the limit
+ * pipelines, the grid barriers of the cooperative getrf panel) is bounded: by the SM's cycle counter, 2 cycles per nanosecond of the limit
  * set here (default 2 s), i.e. at least that long at SM clocks up to 2 GHz. A wait that
  * runs out records RC_ERR_TIMEOUT and where it happened (kernel * 100 + role * 10 + CTA
  * rank in its cluster; kernels 1 = tcgen05 GEMM, 2 = CTA-pair GEMM, 3 = int8 product,
- * 4 = int8 digit-product trailing update,
+ * 4 = int8 digit-product trailing update, 5 = getrf panel grid barrier (site 500),
  * 9 = self-test; roles 0 = loads, 1 = MMAs, 2 = epilogue) in a per-device error word and
  * its kernel returns, leaving the context usable. The word is sticky: while it is set,
  * every tensor-core kernel returns at once and waits in flight give up, and
