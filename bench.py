@@ -10,8 +10,13 @@ GPU by torch -- input generation only, outside every timed region).
 metric unit: TFLOP/s counted as n^3/3 + 2 n^2 nrhs per solve (refinement flops are not
 credited), for the mixed solve and the plain FP64 solve alike.
 
+Beside the headline (single GPU): the same solve at kappa = 1e10 with the emulated-FP64
+factor (--precision emu64: FP64 working copy, int8 digit-product trailing updates) against
+cuSOLVER on that system ("kappa_1e10"), and the roofline of the digit-product kernel.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--n 32768] [--nrhs 64] [--kappa 1e2] [--precision tf32|bf16]
+                    [--n 32768] [--nrhs 64] [--kappa 1e2] [--precision tf32|bf16|emu64]
+                    [--no-e2e] [--no-kappa10] [--no-cpu]
 
 --impl reference times the reference's own CPU path (Remora's cholesky_decomposition +
 solve, compiled from its headers into oracle/_ref) on the host cores, on a bounded
