@@ -66,3 +66,22 @@ def test_argument_checks_of_factorisations_and_sliced_product():
     assert lib.rc_gemm_f64_sliced(10, 4, 10, 1.0, fake, 9, fake, 10, 0.0, fake, 10, None) == 1  # lda < m
     assert lib.rc_gemm_f64_sliced(10, 65, 10, 1.0, fake, 10, fake, 10, 0.0, fake, 10, None) == 4  # > 64 columns
     assert lib.rc_gemm_f64_sliced(0, 4, 10, 1.0, None, 1, None, 1, 0.0, None, 1, None) == 0  # empty
+
+
+def test_mixed_workspace_sizes_without_a_gpu():
+    """rc_spd_solve_mixed_workspace is host arithmetic: the EMU64 solve keeps an FP64 working
+    copy (8 n^2 bytes) where TF32 keeps an FP32 one (4 n^2), panel widths above 4096 fall
+    back to 1024 for EMU64, and every size grows with the right-hand sides."""
+    lib = remora_b200.lib()
+
+    def size(prec, n, nrhs, outer=1024):
+        o = _lib.MixedOptions(1e-15, 100, outer, -1.0)
+        out = ctypes.c_size_t(0)
+        assert lib.rc_spd_solve_mixed_workspace(prec, n, nrhs, ctypes.byref(o), ctypes.byref(out)) == 0
+        return out.value
+
+    n = 4096
+    tf32, emu = size(_lib.RC_PREC_TF32, n, 64), size(_lib.RC_PREC_EMU64, n, 64)
+    assert emu - tf32 >= 3 * n * n  # FP64 instead of FP32 working copy (less the FP32-only buffers)
+    assert size(_lib.RC_PREC_EMU64, n, 64, outer=8192) == size(_lib.RC_PREC_EMU64, n, 64, outer=1024)
+    assert size(_lib.RC_PREC_EMU64, n, 64) > size(_lib.RC_PREC_EMU64, n, 8)
