@@ -51,3 +51,36 @@ def test_max_over_ranks_without_process_group():
     sys.path.insert(0, str(ROOT))
     import bench
     assert bench.max_over_ranks(3.25) == 3.25
+
+
+def test_reference_arm_line_on_rank_0():
+    """The reference arm's JSON line on rank 0 carries the keys the bench contract names, with
+    the sample it timed in its config and no host-device bytes."""
+    import json
+    sys.path.insert(0, str(ROOT))
+    import bench
+    import oracle
+    try:
+        oracle.Reference()
+    except FileNotFoundError:
+        pytest.skip("reference CPU path not built on this machine")
+
+    class Args:
+        ref_n, n, nrhs, steps, warmup, gpus = 96, 32768, 4, 2, 1, 1
+
+    buf = io.StringIO()
+    os.environ.pop("RANK", None)
+    with redirect_stdout(buf):
+        bench.run_reference_arm(Args())
+    lines = buf.getvalue().strip().splitlines()
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
+    assert line["config"]["n"] == 96 and line["config"]["headline_n"] == 32768
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] == 1
+    assert line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
