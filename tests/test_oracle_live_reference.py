@@ -133,3 +133,36 @@ def test_cholesky_solve_random(orc, ref, order):
         assert orc.cholesky_solve(A.copy(order="A"), X1) == 0
         assert ref.cholesky_solve(A.copy(order="A"), X2) == 0
         assert oracle.rel_fro(X1, X2) <= 1e-12, (n, r)
+
+
+@pytest.mark.parametrize("dtype,order", CASES)
+def test_blas2_and_trmm_random_shapes(orc, ref, dtype, order):
+    rs = np.random.default_rng(17)
+    for n, r in ((1, 1), (37, 5), (130, 40)):
+        A = _arr(rs, (n, n + 3), dtype, order)
+        x = _arr(rs, (n + 3,), dtype, "C")
+        y1 = _arr(rs, (n,), dtype, "C")
+        y2 = y1.copy()
+        orc.gemv(A, x, y1, alpha=1.5)
+        ref.gemv(A, x, y2, alpha=1.5)
+        assert oracle.rel_fro(y1, y2) <= TOL[dtype], n
+        for upper in (False, True):
+            for unit in (False, True):
+                T = _arr(rs, (n, n), dtype, order) + n * np.eye(n, dtype=dtype)
+                T = np.array(np.triu(T) if upper else np.tril(T), dtype=dtype, order=order)
+                for left in (True, False):
+                    v1 = _arr(rs, (n,), dtype, "C")
+                    v2 = v1.copy()
+                    assert orc.trsv(T, v1, upper=upper, unit=unit, left=left) == 0
+                    ref.trsv(T, v2, upper=upper, unit=unit, left=left)
+                    assert oracle.rel_fro(v1, v2) <= TOL[dtype], (n, upper, unit, left)
+                v1 = _arr(rs, (n,), dtype, "C")
+                v2 = v1.copy()
+                orc.trmm(T, v1.reshape(n, 1), upper=upper, unit=unit)
+                ref.trmv(T, v2, upper=upper, unit=unit)
+                assert oracle.rel_fro(v1, v2) <= TOL[dtype], (n, upper, unit)
+                B1 = _arr(rs, (n, r), dtype, order)
+                B2 = B1.copy(order="A")
+                orc.trmm(T, B1, upper=upper, unit=unit)
+                ref.trmm(T, B2, upper=upper, unit=unit)
+                assert oracle.rel_fro(B1, B2) <= TOL[dtype], (n, r, upper, unit)
