@@ -166,3 +166,27 @@ def test_blas2_and_trmm_random_shapes(orc, ref, dtype, order):
                 orc.trmm(T, B1, upper=upper, unit=unit)
                 ref.trmm(T, B2, upper=upper, unit=unit)
                 assert oracle.rel_fro(B1, B2) <= TOL[dtype], (n, r, upper, unit)
+
+
+def test_rng_blocks_at_random_offsets(orc, ref):
+    """Fills of 3 x 8 blocks at random row/column offsets (around the 16-bit counter masks
+    and past 2^32) under random keys, against the reference's own per-group device functions
+    compiled as host code (counter of group (i, j): kernels/hip/random.hpp:167). Host libm on
+    both sides, so the float transforms are compared bit for bit as well."""
+    rs = np.random.default_rng(18)
+    offsets = [(0, 0), (65534, 65532), (2**32 - 1, 4), (12345, 2**32 + 8), (2**40 + 7, 2**33 + 65536)]
+    offsets += [(int(rs.integers(0, 2**48)), 4 * int(rs.integers(0, 2**40))) for _ in range(6)]
+    for row0, col0 in offsets:
+        key = [int(v) for v in rs.integers(0, 2**32, 4)]
+        got = {k: orc.rng_fill(k, key, 3, 8, True, -1.5, 2.5, ia=-4, ib=9, row0=row0, col0=col0)
+               for k in ("uniform", "normal", "discrete_f32")}
+        for i in range(3):
+            for j in range(0, 8, 4):
+                r, c = row0 + i, col0 + j
+                ctr = [r & 0xFFFF, (r >> 32) & 0xFFFFFFFF, c & 0xFFFF, (c >> 32) & 0xFFFFFFFF]
+                x = ref.threefry(ctr, key)
+                want = {"uniform": ref.uniform4(-1.5, 2.5, x), "normal": ref.normal4(-1.5, 2.5, x),
+                        "discrete_f32": [v - 4 for v in ref.discrete4(key, ctr, 14)]}
+                for k, w in want.items():
+                    a = np.asarray(got[k][i, j:j + 4], dtype=np.float32)
+                    assert np.array_equal(a.view(np.uint32), np.asarray(w, np.float32).view(np.uint32)), (k, r, c)
