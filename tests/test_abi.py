@@ -5,6 +5,8 @@ import ctypes
 import re
 from pathlib import Path
 
+import pytest
+
 import remora_b200
 from remora_b200 import _lib
 
@@ -85,3 +87,18 @@ def test_mixed_workspace_sizes_without_a_gpu():
     assert emu - tf32 >= 3 * n * n  # FP64 instead of FP32 working copy (less the FP32-only buffers)
     assert size(_lib.RC_PREC_EMU64, n, 64, outer=8192) == size(_lib.RC_PREC_EMU64, n, 64, outer=1024)
     assert size(_lib.RC_PREC_EMU64, n, 64) > size(_lib.RC_PREC_EMU64, n, 8)
+
+
+@pytest.mark.parametrize("compiler,std", [("gcc", "-std=c99"), ("g++", "-std=c++14")])
+def test_c_abi_header_is_plain_c_and_cpp(tmp_path, compiler, std):
+    """include/remora_cuda.h compiles on its own as C99 and as C++14 (no CUDA headers, no
+    torch types), which is what an FFI binding or a g++-built Remora program includes."""
+    import shutil
+    import subprocess
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} not installed")
+    src = tmp_path / ("t.c" if compiler == "gcc" else "t.cpp")
+    src.write_text('#include <remora_cuda.h>\nint main(void) { return rc_version() > 0 ? 0 : 1; }\n')
+    inc = Path(__file__).resolve().parent.parent / "include"
+    subprocess.run([compiler, std, "-Wall", "-Werror", "-pedantic", "-fsyntax-only", f"-I{inc}", str(src)],
+                   check=True)
