@@ -102,3 +102,14 @@ def test_c_abi_header_is_plain_c_and_cpp(tmp_path, compiler, std):
     inc = Path(__file__).resolve().parent.parent / "include"
     subprocess.run([compiler, std, "-Wall", "-Werror", "-pedantic", "-fsyntax-only", f"-I{inc}", str(src)],
                    check=True)
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """Without the built library every entry point raises (the ops wrappers all load it
+    through _lib.lib()): there is no CPU fallback."""
+    monkeypatch.setattr(_lib, "LIB_PATH", tmp_path / "libremora_cuda.so")
+    monkeypatch.setattr(_lib, "_lib", None)
+    with pytest.raises(RuntimeError, match="is missing"):
+        _lib.lib()
+    with pytest.raises(RuntimeError, match="is missing"):
+        _lib.call("rc_potrf_f64", 0, 4, None, 4, None, None)
